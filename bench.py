@@ -1,0 +1,395 @@
+"""Benchmark of the LDDMM registration hot path on B200.
+
+Workload (default): one 3D sphere -> cube registration -- icosphere radius 1,
+4 subdivisions (2562 vertices / 5120 triangles) onto the surface of [-1,1]^3 with a
+32 x 32 quad grid per face (12288 triangles), Matern nu=3/2 deformation kernel width
+0.4, varifold Gaussian(0.15) x Binet, 20 time steps, L-BFGS memory 5, at most 500
+iterations (tolerance 1e-6, Wolfe 1e-4 / 0.9), zero initial momenta.  One "step" is
+one whole registration.  Synthetic data, generated deterministically.
+
+Metric: registrations/s (whole job, all ranks); the JSON line also reports pair
+interactions/s, the objective's relative error against the FP64 oracle at the
+returned point, the FP32 roofline of the dominant sweep, and the reference's C++
+path timed on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun: every rank runs its own registration (independent
+replicas, no data-path collective); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "registrations/s at 1e-5 rel. objective; Gpair-interactions/s vs FP32 peak"
+UNIT = "registrations/s"
+WORKLOAD = "sphere2cube: icosphere 2562 v / 5120 t -> cube 12288 t, Matern nu=3/2 w=0.4, " \
+           "varifold G(0.15) x Binet, T=20, L-BFGS m=5, <=500 iterations"
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+# Objective evaluations of one registration of this workload, used to turn the
+# reference's per-evaluation CPU time into registrations/s (the reference cannot run
+# a whole registration inside the bench's time budget).  Measured by this bench on
+# B200 (FP32 path, 500 iterations); the FP64 path takes a similar count.
+EVALS_PER_REGISTRATION = 520
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--itr", type=int, default=500)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload():
+    from lddmm_b200 import problem
+
+    return problem.sphere_to_cube()
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        try:
+            with open(self.f.name) as fh:
+                for line in fh:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        finally:
+            os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4)
+                          if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------- reference (CPU) arm
+
+def _ref_eval_worker(args):
+    """One objgrd evaluation of the workload by the reference's C++ path (compiled
+    from its own sources into oracle/_ref), or by the oracle port when that build is
+    absent.  Returns (seconds, kind)."""
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    from oracle.oracle import Oracle, Reference
+
+    P = workload()
+    alp = np.random.default_rng(0).normal(size=P.var_num) * 0.01
+    if Reference.available(3):
+        R, kind = Reference(3), "reference"
+    else:
+        R, kind = Oracle(threads=1), "port"
+    t0 = time.perf_counter()
+    R.objgrd(P, alp)
+    return time.perf_counter() - t0, kind
+
+
+def mem_available_gb() -> float:
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 16.0
+
+
+def reference_workers() -> int:
+    # the reference stores an N x N x T kernel stack: ~1.05 GB per process here
+    return max(1, min(os.cpu_count() or 1, int(mem_available_gb() / 1.6), 64))
+
+
+def run_reference(args):
+    import multiprocessing as mp
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    n = reference_workers()
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(n) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_eval_worker, range(n))
+        t0 = time.perf_counter()
+        times, kinds = [], set()
+        for _ in range(args.steps):
+            out = pool.map(_ref_eval_worker, range(n))
+            times += [t for t, _ in out]
+            kinds |= {k for _, k in out}
+        wall = time.perf_counter() - t0
+    per_eval = statistics.mean(times)
+    value = n / (per_eval * EVALS_PER_REGISTRATION)
+    kind = "reference" if kinds == {"reference"} else "port"
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "sample": "objgrd evaluations"},
+        "cpu_baseline": {
+            "value": value, "unit": UNIT, "cores": n, "kind": kind,
+            "sample": f"{n} processes x one objective+gradient evaluation per step "
+                      f"(mean {per_eval:.2f} s), scaled by {EVALS_PER_REGISTRATION} "
+                      f"evaluations per registration"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- our arm
+
+def run_ours(args):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from lddmm_b200 import _lib, api
+
+    P = workload()
+    stream = torch.cuda.current_stream()
+    ctx = api.Context(P, stream=stream.cuda_stream, device=local)
+    nvar = ctx.var_total
+    d_alp = torch.zeros(nvar, dtype=torch.float64, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    opt = _lib.Opt(args.itr, 1e-6, 1e-4, 0.9, 5, 0, 0.0)
+    res = (_lib.Result * 1)()
+
+    def registration():
+        d_alp.zero_()
+        rc = _lib.lib.lddmm_lbfgs_device(ctx.handle, C.byref(opt), C.c_void_p(d_alp.data_ptr()),
+                                         res)
+        if rc < 0:
+            _lib.check(rc)
+        return ctx.counters()
+
+    for _ in range(max(args.warmup, 0)):
+        flush.zero_()
+        registration()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches = 0
+    evals = 0
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t_start.record(stream)
+        for _ in range(args.steps):
+            flush.zero_()
+            c = registration()
+            launches += c["launches"]
+            evals += c["evals"]
+        t_end.record(stream)
+        torch.cuda.synchronize()
+    ms = t_start.elapsed_time(t_end)
+    if dist:
+        dist.barrier()
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    clocks = clk.summary()
+    r = res[0]
+    x = d_alp.cpu().numpy()
+    iters, status, f_final = r.iters, r.status, r.fcn
+
+    # e2e: the reference-facing single call (MEX LDDMM3D equivalent) on HOST buffers,
+    # context creation, host<->device copies and the whole registration inside.
+    ini = np.ascontiguousarray(P.ini_nde)
+    alp0 = np.zeros(nvar)
+    out = np.zeros(nvar)
+    ifo = P.elm_ifo  # rows x N, one contiguous column per vertex (getElmIfo layout)
+    L = _lib.lib
+
+    def e2e_call():
+        return L.lddmm_LDDMM(3, P.nde_num, P.dfm_elm_num, P.elm_ifo.shape[1], P.tgt_elm_num,
+                             _lib.dptr(ini), _lib.dptr(alp0), _lib.iptr(P.elm_vtx),
+                             _lib.iptr(ifo), _lib.dptr(P.tgt_cen), _lib.dptr(P.tgt_vol),
+                             _lib.dptr(P.tgt_dir), b"G", P.cen_width, b"B", P.dir_width,
+                             P.dis_wgt, P.knl_order, P.knl_width, P.time_stp, P.time_num,
+                             args.itr, 1e-6, 1e-4, 0.9, 5, 0, _lib.dptr(out))
+
+    e2e_call()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    e_steps = max(1, min(args.steps, 3))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        _lib.check(min(e2e_call(), 0))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e_ms = float(t.item())
+    h2d = (ini.nbytes + alp0.nbytes + P.elm_vtx.nbytes + ifo.nbytes + P.tgt_cen.nbytes
+           + P.tgt_dir.nbytes + P.tgt_vol.nbytes)
+    d2h = out.nbytes
+
+    # roofline of the dominant sweep: live per-launch timing (CUDA events on the
+    # context stream) of one evaluation at the returned point
+    sweeps = ctx.time_sweeps(reps=5)
+    peak = C.c_double()
+    _lib.check(L.lddmm_fp32_peak(local, C.byref(peak)))
+    T, N, Ed, Et = P.T, P.nde_num, P.dfm_elm_num, P.tgt_elm_num
+    fl = {k: L.lddmm_flops_per_pair(i, 3, P.knl_order, b"G", b"B")
+          for i, k in enumerate(("shoot", "adjoint", "varifold"))}
+    pairs_launch = {"shoot": N * N, "adjoint": N * N, "varifold": Ed * (Ed + Et)}
+    per_eval_ms = {"shoot": T * sweeps["shoot"], "adjoint": T * sweeps["adjoint"],
+                   "varifold": sweeps["varifold"]}
+    dom = max(per_eval_ms, key=per_eval_ms.get)
+    achieved = pairs_launch[dom] * fl[dom] / (sweeps[dom] * 1e-3) / 1e12
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as fh:
+            traffic = json.load(fh).get(dom)
+    except (OSError, ValueError):
+        pass
+
+    pairs_per_eval = 2 * T * N * N + Ed * (Ed + Et)
+    evals_per_reg = evals / max(args.steps, 1)
+    regs = args.steps * world
+    value = regs / (ms * 1e-3)
+    gpairs = (evals * pairs_per_eval + args.steps * Et * Et) * world / (ms * 1e-3) / 1e9
+
+    # accuracy at the returned point against the FP64 oracle (rank 0)
+    rel_f = None
+    cpu = None
+    if rank == 0:
+        from oracle.oracle import Oracle, Reference
+
+        orc = Oracle(threads=min(os.cpu_count() or 1, 32))
+        with api.Context(P) as c2:
+            fg, _ = c2.objgrd(x)
+        fo, _ = orc.objgrd(P, x)
+        rel_f = abs(fg[0] - fo) / abs(fo)
+        if world == 1 and not args.no_cpu_baseline:
+            alp = np.random.default_rng(0).normal(size=P.var_num) * 0.01
+            if Reference.available(3):
+                R, kind = Reference(3), "reference"
+            else:
+                R, kind = Oracle(threads=1), "port"
+            t0 = time.perf_counter()
+            R.objgrd(P, alp)
+            te = time.perf_counter() - t0
+            cpu = {"value": 1.0 / (te * EVALS_PER_REGISTRATION), "unit": UNIT, "cores": 1,
+                   "kind": kind,
+                   "sample": f"one objective+gradient evaluation ({te:.2f} s, single "
+                             f"thread) scaled by {EVALS_PER_REGISTRATION} evaluations "
+                             f"per registration"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 kernels + f64 optimiser", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}",
+                       "l2": "256 MiB memset before every registration",
+                       "iters": iters, "status": status, "evals_per_registration": evals_per_reg,
+                       "f_final": f_final, "rel_err_f_vs_fp64_oracle": rel_f,
+                       "gpair_interactions_per_s": gpairs,
+                       "cluster": list(ctx.launch_config()),
+                       "sweep_ms": {k: round(v, 5) for k, v in sweeps.items()}},
+            "roofline": {"bound": "fp32", "kernel": f"{dom} sweep", "achieved": achieved,
+                         "peak": peak.value, "unit": "TFLOP/s", "frac": achieved / peak.value,
+                         "peak_source": "measured FP32 FMA probe (lddmm_fp32_peak), same GPU",
+                         "flops_per_pair": fl[dom], "pairs_per_launch": pairs_launch[dom],
+                         "traffic": traffic},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e_steps / (e_ms * 1e-3) * world, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "call": "lddmm_LDDMM (host buffers; context set-up inside)"},
+            "gpu_launches": launches,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

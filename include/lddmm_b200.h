@@ -1,0 +1,212 @@
+/*
+ * lddmm_b200 -- C ABI of the B200 (sm_100a) LDDMM landmark/surface registration
+ * with varifold matching.
+ *
+ * These entry points replace the routines the reference's C++/MATLAB drivers hand
+ * to L-BFGS (dnhsieh/LDDMM, Cpp/src):
+ *
+ *   lddmm_objgrd      <- void objgrd(double *fcnVal, double *grdStk, double *alpStk,
+ *                                    fcndata &)                    Cpp/src/objgrd.cpp:26
+ *   lddmm_lbfgs       <- int LBFGS(double *fcnNow, double *grdNow, double *posNow,
+ *                                  optdata &, fcndata &)           Cpp/src/LBFGS.cpp:25
+ *                        (with lineSearch, Cpp/src/lineSearch.cpp:26, and
+ *                         getDirection, Cpp/src/getDirection.cpp:9, on the device)
+ *   lddmm_LDDMM       <- MEX LDDMM2D/LDDMM3D(iniNdeMat, iniAlpVec, ..., Verbose)
+ *                                                                  Cpp/src/LDDMM.cpp:11-46
+ *   lddmm_shoot       <- computeNodePosition.m (trajectory and velocities)
+ *                                                                  Cpp/src/computeNodePosition.m:1
+ *   lddmm_elm_ifo     <- getElmIfo.m                               Cpp/src/getElmIfo.m:1
+ *   lddmm_multiply_kernel <- multiplyKernel (MEX multiplyKernelITF) Cpp/src/multiplyKernel.cpp:22
+ *   lddmm_dq_kernel   <- dqKernel                                  Cpp/src/dqKernel.cpp:31
+ *   lddmm_varifold    <- varifoldITF / varifold (gradient overload) Cpp/src/varifoldITF.cpp:7
+ *
+ * Layout is the reference's C++ one: coordinates fastest, then node, then time
+ * step (Cpp/src/objgrd.cpp:47-50); element and adjacency tables are 0-based int32
+ * (Cpp/src/LDDMM.m:7-8).  All buffers passed to entry points without the _device
+ * suffix are host memory owned by the caller; a context owns all device memory,
+ * its CUDA stream and its CUDA graphs.
+ *
+ * Return codes: 0 success; 1/2/3 line-search failure codes of the reference
+ * (not a descent direction / function may be unbounded below / bracketed but the
+ * weak Wolfe conditions not satisfied, Cpp/src/lineSearch.cpp:45,101,109); negative
+ * values are errors (LDDMM_ERR_*), with a message from lddmm_last_error().
+ * No entry point calls exit() or prints unless asked to (verbose).
+ *
+ * Threading: a context is used by one host thread at a time; distinct contexts are
+ * independent.  The library keeps no mutable global state besides the per-thread
+ * error message.
+ */
+#ifndef LDDMM_B200_H
+#define LDDMM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LDDMM_OK 0
+#define LDDMM_LS_NOT_DESCENT 1
+#define LDDMM_LS_UNBOUNDED 2
+#define LDDMM_LS_BRACKET 3
+#define LDDMM_ERR_ARG (-1)
+#define LDDMM_ERR_CUDA (-2)
+#define LDDMM_ERR_NONFINITE (-3)
+#define LDDMM_ERR_TIMEOUT (-4)
+#define LDDMM_ERR_NOMEM (-5)
+#define LDDMM_ERR_UNSUPPORTED (-6)
+
+typedef struct lddmm_ctx lddmm_ctx;
+
+/* One registration pair: the fields of `parameters` and `discrepancy`
+ * (Cpp/src/struct.h:25-56) plus the sizes the MEX reads from its arrays
+ * (Cpp/src/LDDMM.cpp:44-52). */
+typedef struct lddmm_problem {
+	int dim;                  /* DIMNUM: 2 or 3 */
+	int nde_num;              /* ndeNum: landmarks N */
+	int time_num;             /* timeNum: time points; T = time_num - 1 Euler steps */
+	double time_stp;          /* timeStp */
+	int knl_order;            /* knlOrder: -1 Gaussian, 0..4 Matern */
+	double knl_width;         /* knlWidth */
+	const double *ini_nde;    /* iniNdeMat: dim x N */
+	double dis_wgt;           /* disWgt */
+	int dfm_elm_num;          /* dfmElmNum */
+	const int *dfm_elm_vtx;   /* dfmElmVtxMat: dim x E_d, 0-based */
+	int dfm_elm_ifo_num;      /* dfmElmIfoNum: rows of dfmElmIfoMat (0: computed) */
+	const int *dfm_elm_ifo;   /* dfmElmIfoMat: rows x N, or NULL to compute it */
+	int tgt_elm_num;          /* tgtElmNum */
+	const double *tgt_cen_pos;/* tgtCenPosMat: dim x E_t */
+	const double *tgt_uni_dir;/* tgtUniDirMat: dim x E_t */
+	const double *tgt_elm_vol;/* tgtElmVolVec: E_t */
+	char cen_knl_type;        /* cenKnlType: 'G' Gaussian, 'C' Cauchy */
+	double cen_knl_width;     /* cenKnlWidth */
+	char dir_knl_type;        /* dirKnlType: 'B' Binet, 'L' linear, 'O'/'U' Gaussian */
+	double dir_knl_width;     /* dirKnlWidth */
+} lddmm_problem;
+
+/* Optimiser options: the fields of `optdata` (Cpp/src/struct.h:4-23). */
+typedef struct lddmm_opt {
+	int itr_max;              /* itrMax (MaxIterations) */
+	double tol_val;           /* tolVal (OptimalityTolerance): stop when |g| < tol */
+	double wolfe1;            /* Armijo constant */
+	double wolfe2;            /* curvature constant */
+	int mem_num;              /* memNum (Columns), at most 32 */
+	int vbs_flg;              /* print the reference's iteration table per pair */
+	double rel_obj_tol;       /* additional stop: |f_prev - f| <= rel_obj_tol |f_prev|;
+	                             0 disables (the reference has only the |g| test) */
+} lddmm_opt;
+
+/* Launch configuration.  Zero fields take defaults / the autotuner's choice. */
+typedef struct lddmm_config {
+	int cluster_shoot;        /* CTAs per i-tile (thread-block cluster size, 1..8) */
+	int cluster_adjoint;
+	int cluster_varifold;
+	int autotune;             /* 1: time the candidate cluster sizes at creation */
+	int use_graph;            /* 1 (default): capture the L-BFGS cycle in a CUDA graph */
+	void *stream;             /* cudaStream_t to run on; NULL: the context creates one */
+	int device;               /* CUDA device ordinal (default 0) */
+} lddmm_config;
+
+/* Per-pair outcome of lddmm_lbfgs. */
+typedef struct lddmm_result {
+	double fcn;               /* objective at the returned point */
+	double grd_len;           /* |g| there */
+	int status;               /* 0, 1, 2, 3 or an LDDMM_ERR_* value */
+	int iters;                /* accepted L-BFGS iterations */
+	int evals;                /* objective evaluations */
+	int pad_;
+} lddmm_result;
+
+const char *lddmm_last_error(void);
+const char *lddmm_version(void);
+
+/* Context over `num` independent pairs (a batch; num = 1 for one registration).
+ * All pairs must share dim, time_num, knl_order, cen_knl_type and dir_knl_type.
+ * Replaces the workspace set-up of Cpp/src/LDDMM.cpp:54-80. */
+int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm_config *cfg,
+                     lddmm_ctx **out);
+void lddmm_ctx_destroy(lddmm_ctx *ctx);
+int lddmm_ctx_num_pairs(const lddmm_ctx *ctx);
+/* Variables of pair `pair` (dim * N * (time_num - 1)) and their offset in the
+ * concatenated vectors every batched entry point uses. */
+long long lddmm_ctx_var_num(const lddmm_ctx *ctx, int pair);
+long long lddmm_ctx_var_offset(const lddmm_ctx *ctx, int pair);
+long long lddmm_ctx_var_total(const lddmm_ctx *ctx);
+/* The cudaStream_t the context runs on. */
+void *lddmm_ctx_stream(const lddmm_ctx *ctx);
+/* Cluster sizes in use (after autotuning): out[0..2] = shoot, adjoint, varifold. */
+int lddmm_ctx_launch_config(const lddmm_ctx *ctx, int *out3);
+
+/* Objective and gradient of every pair at alp (concatenated, host memory);
+ * fcn[num], grd like alp.  objgrd.cpp:26 semantics. */
+int lddmm_objgrd(lddmm_ctx *ctx, const double *alp, double *fcn, double *grd);
+/* Same on device buffers (no host copies, synchronous on the context stream unless
+ * `async` is set). */
+int lddmm_objgrd_device(lddmm_ctx *ctx, const double *d_alp, double *d_fcn, double *d_grd,
+                        int async);
+
+/* L-BFGS from alp_inout (host) for every pair; on return alp_inout holds each pair's
+ * last accepted point (the reference's posNow) and res[num] the outcome.  Returns 0
+ * when every pair ended with status 0, else the first nonzero status. */
+int lddmm_lbfgs(lddmm_ctx *ctx, const lddmm_opt *opt, double *alp_inout, lddmm_result *res);
+int lddmm_lbfgs_device(lddmm_ctx *ctx, const lddmm_opt *opt, double *d_alp_inout,
+                       lddmm_result *res);
+/* Per-iteration record of pair `pair` from the last lddmm_lbfgs call: rows of
+ * (f, |g|, step length, evaluations in the line search), row 0 the initial point.
+ * Returns the number of rows written (at most cap). */
+int lddmm_lbfgs_trace(const lddmm_ctx *ctx, int pair, double *rows4, int cap);
+
+/* Trajectory of every pair: nde_stk (dim x N x time_num per pair) and velocities
+ * vlc_stk (dim x N x (time_num - 1) per pair), concatenated by pair.  Either output
+ * may be NULL. */
+int lddmm_shoot(lddmm_ctx *ctx, const double *alp, double *nde_stk, double *vlc_stk);
+
+/* The whole MEX entry point LDDMM2D/LDDMM3D (Cpp/src/LDDMM.cpp:11-98) for one pair:
+ * same 22 arguments in the same order, plus the array sizes MATLAB would supply and
+ * the output buffer optAlpVec (dim * N * (timeNum - 1)).  dfmElmIfoMat may be NULL.
+ * Returns LBFGS's code like the reference (0, or the line-search code). */
+int lddmm_LDDMM(int dim, int nde_num, int dfm_elm_num, int dfm_elm_ifo_num, int tgt_elm_num,
+                const double *iniNdeMat, const double *iniAlpVec, const int *dfmElmVtxMat,
+                const int *dfmElmIfoMat, const double *tgtCenPosMat, const double *tgtElmVolVec,
+                const double *tgtUniDirMat, char cenKnlType, double cenKnlWidth,
+                char dirKnlType, double dirKnlWidth, double disWgt, int knlOrder,
+                double knlWidth, double timeStp, int timeNum, int MaxIterations,
+                double OptimalityTolerance, double Wolfe1, double Wolfe2, int Columns,
+                int Verbose, double *optAlpVec);
+
+/* getElmIfo (Cpp/src/getElmIfo.m): vertex -> adjacent element table.  elm_vtx is
+ * vpe x elm_num (0-based).  With ifo == NULL returns the row count; otherwise fills
+ * rows x nde_num and returns the row count.  Negative on bad input. */
+int lddmm_elm_ifo(const int *elm_vtx, int vpe, int elm_num, int nde_num, int *ifo);
+
+/* Single kernel sums on the GPU (host buffers; a temporary device workspace):
+ * v_i = sum_j K(q_i, q_j) a_j                    (multiplyKernel.cpp:22)
+ * dq_i = sum_j (l_i.r_j + l_j.r_i) dK/dq_i       (dqKernel.cpp:31)
+ * V, dV/dq of the varifold discrepancy           (varifold3D.cpp:410, varifold2D.cpp:378) */
+int lddmm_multiply_kernel(int dim, int n, const double *q, const double *a, int knl_order,
+                          double knl_width, double *v);
+int lddmm_dq_kernel(int dim, int n, const double *q, const double *l, const double *r,
+                    int knl_order, double knl_width, double *dq);
+int lddmm_varifold(const lddmm_problem *prob, const double *nde, double *val, double *dq);
+
+/* Measurement.  Evaluates the objective `reps` times at the context's current
+ * trial point with CUDA events on the context stream around every sweep launch and
+ * writes average milliseconds per launch: ms4[0] shooting step, ms4[1] fused adjoint
+ * step, ms4[2] varifold sweep, ms4[3] whole evaluation. */
+int lddmm_ctx_time_sweeps(lddmm_ctx *ctx, int reps, double *ms4);
+/* Counters of the last lddmm_lbfgs call: out[0] L-BFGS cycles launched, out[1]
+ * kernels per cycle, out[2] kernel launches in total, out[3] objective evaluations
+ * summed over pairs.  Returns the number of values written (at most n). */
+int lddmm_ctx_counters(const lddmm_ctx *ctx, long long *out, int n);
+
+/* FP32 FMA throughput of this GPU (TFLOP/s, FMA = 2 flops) measured by a probe
+ * kernel of independent FMA chains over every SM; the roofline denominator of the
+ * FP32-bound sweeps.  Returns 0 and writes the figure to *tflops. */
+int lddmm_fp32_peak(int device, double *tflops);
+
+/* FLOPs per pair interaction the roofline uses (FMA = 2, as executed), for the
+ * shooting step, the fused adjoint step and the varifold pair of the given kinds. */
+double lddmm_flops_per_pair(int sweep, int dim, int knl_order, char cen_type, char dir_type);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

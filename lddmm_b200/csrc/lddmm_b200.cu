@@ -1,0 +1,1410 @@
+// Host runtime of the B200 LDDMM library: batch layout, device memory, kernel
+// dispatch, the objective sweep, the device L-BFGS cycle (CUDA graph) and the C ABI.
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lddmm_b200.h"
+#include "common.cuh"
+#include "kernels.cuh"
+#include "layout.h"
+#include "lbfgs.cuh"
+#include "ops.cuh"
+#include "sweep.cuh"
+
+using namespace lddmm;
+
+namespace {
+
+thread_local std::string g_err;
+
+void set_err(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+#define CU(expr)                                                                    \
+  do {                                                                              \
+    cudaError_t e_ = (expr);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      set_err("%s:%d %s: %s", __FILE__, __LINE__, #expr, cudaGetErrorString(e_));   \
+      return LDDMM_ERR_CUDA;                                                        \
+    }                                                                               \
+  } while (0)
+
+#define CUE(expr)                 \
+  do {                            \
+    cudaError_t e_ = (expr);      \
+    if (e_ != cudaSuccess) return e_; \
+  } while (0)
+
+constexpr int kWarps = 4;  // warps per sweep CTA
+
+template <class T>
+cudaError_t dalloc(T **p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e == cudaSuccess) e = cudaMemset(*p, 0, n * sizeof(T));
+  return e;
+}
+
+int pad_to(int n, int k) { return (n + k - 1) / k * k; }
+
+}  // namespace
+
+// ============================================================== the context
+
+struct lddmm_ctx {
+  int D = 3, order = -1, T = 0, time_num = 0, P = 0;
+  char ct = 'G', dt = 'B';
+  bool has_vfd = true;
+  float ow2 = 0.0f;
+  int device = 0;
+  std::vector<PairDesc> hpd;
+  int NPtot = 0, EDtot = 0, ETtot = 0, ntile_tot = 0, netile_tot = 0, nchunk_tot = 0;
+  long long nvar = 0;
+  int n_pt_items = 0, n_el_items = 0;
+  int S_shoot = 1, S_adj = 1, S_vfd = 1;
+
+  // device memory
+  PairDesc *pd = nullptr;
+  int *act = nullptr;
+  PairState *st = nullptr;
+  float4 *qs = nullptr, *as = nullptr, *us = nullptr, *ls = nullptr;
+  double *q64 = nullptr, *p64 = nullptr;
+  float4 *ec = nullptr, *en = nullptr, *tc = nullptr, *tn = nullptr;
+  double *e64 = nullptr, *dcdd = nullptr, *tgt64 = nullptr;
+  int4 *elm = nullptr;
+  int *pt_pair = nullptr, *adj_ptr = nullptr;
+  int4 *adj = nullptr;
+  double *reg_part = nullptr, *vfd_part = nullptr, *f_dev = nullptr;
+  int2 *pt_items = nullptr, *el_items = nullptr;
+  int *chunk_pair = nullptr;
+  double *X = nullptr, *G = nullptr, *XT = nullptr, *GT = nullptr, *Dv = nullptr, *Qv = nullptr;
+  double *Sh = nullptr, *Yh = nullptr;
+  int m_alloc = 0;
+  double *part[2] = {nullptr, nullptr};
+  double *rec = nullptr;
+  int rec_cap = 0;
+
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  long long last_cycles = 0, last_launches = 0, last_evals = 0;
+  bool use_graph = true;
+  cudaGraphExec_t cycle_exec = nullptr;
+  OptParams graph_opt{};
+  bool graph_valid = false;
+
+  // dispatch
+  cudaError_t (*shoot)(lddmm_ctx &, int t, double *vlc) = nullptr;
+  cudaError_t (*adjoint)(lddmm_ctx &, int t, double *g, double *pdot) = nullptr;
+  cudaError_t (*varifold)(lddmm_ctx &) = nullptr;
+  cudaError_t (*tt)(lddmm_ctx &, int p, double *part, int nblk, double cw, double dw) = nullptr;
+
+  ~lddmm_ctx();
+};
+
+template <class T>
+static void dfree(T *&p) {
+  if (p) cudaFree((void *)p);
+  p = nullptr;
+}
+
+lddmm_ctx::~lddmm_ctx() {
+  if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
+  dfree(pd); dfree(act); dfree(st); dfree(qs); dfree(as); dfree(us); dfree(ls);
+  dfree(q64); dfree(p64); dfree(ec); dfree(en); dfree(tc); dfree(tn); dfree(e64);
+  dfree(dcdd); dfree(tgt64); dfree(elm); dfree(pt_pair); dfree(adj_ptr); dfree(adj);
+  dfree(reg_part); dfree(vfd_part); dfree(f_dev); dfree(pt_items); dfree(el_items);
+  dfree(chunk_pair); dfree(X); dfree(G); dfree(XT); dfree(GT); dfree(Dv); dfree(Qv);
+  dfree(Sh); dfree(Yh); dfree(part[0]); dfree(part[1]); dfree(rec);
+  if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+// ============================================================ kernel launch
+
+template <class Op>
+static cudaError_t launch_sweep(const Op &op, const int2 *items, int n_items, int S,
+                                cudaStream_t stream) {
+  if (n_items == 0) return cudaSuccess;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(n_items * S));
+  cfg.blockDim = dim3(kWarps * 32);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)S;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, sweep_kernel<Op, kWarps>, op, items, S);
+}
+
+template <int D, int ORDER>
+static cudaError_t shoot_impl(lddmm_ctx &c, int t, double *vlc) {
+  ShootOp<D, ORDER> op;
+  op.pd = c.pd;
+  op.act = c.act;
+  op.qs_t = c.qs + (size_t)t * c.NPtot;
+  op.as_t = c.as + (size_t)t * c.NPtot;
+  op.q64_t = c.q64 + (size_t)t * c.NPtot * D;
+  op.q64_n = c.q64 + (size_t)(t + 1) * c.NPtot * D;
+  op.qs_n = c.qs + (size_t)(t + 1) * c.NPtot;
+  op.x64 = c.XT;
+  op.vlc64 = vlc;
+  op.tile_part = c.reg_part + (size_t)t * c.ntile_tot;
+  op.t = t;
+  return launch_sweep(op, c.pt_items, c.n_pt_items, c.S_shoot, c.stream);
+}
+
+template <int D, int ORDER>
+static cudaError_t adjoint_impl(lddmm_ctx &c, int t, double *g, double *pdot) {
+  AdjointOp<D, ORDER> op;
+  op.pd = c.pd;
+  op.act = c.act;
+  op.qs_t = c.qs + (size_t)t * c.NPtot;
+  op.us_t = c.us + (size_t)(t & 1) * c.NPtot;
+  op.ls_t = c.ls + (size_t)(t & 1) * c.NPtot;
+  op.as_t = c.as + (size_t)t * c.NPtot;
+  op.p64 = c.p64;
+  op.x64 = c.XT;
+  op.g64 = g;
+  op.us_n = (t > 0) ? c.us + (size_t)((t - 1) & 1) * c.NPtot : nullptr;
+  op.ls_n = (t > 0) ? c.ls + (size_t)((t - 1) & 1) * c.NPtot : nullptr;
+  op.pdot64 = pdot;
+  op.t = t;
+  return launch_sweep(op, c.pt_items, c.n_pt_items, c.S_adj, c.stream);
+}
+
+template <int D, char CT, char DT>
+static cudaError_t varifold_impl(lddmm_ctx &c) {
+  VarifoldOp<D, CT, DT> op;
+  op.pd = c.pd;
+  op.act = c.act;
+  op.ec = c.ec;
+  op.en = c.en;
+  op.tc = c.tc;
+  op.tn = c.tn;
+  op.e64 = c.e64;
+  op.dcdd = c.dcdd;
+  op.tile_part = c.vfd_part;
+  op.ow2 = c.ow2;
+  return launch_sweep(op, c.el_items, c.n_el_items, c.S_vfd, c.stream);
+}
+
+template <int D, char CT, char DT>
+static cudaError_t tt_impl(lddmm_ctx &c, int p, double *part, int nblk, double cw, double dw) {
+  const PairDesc &P = c.hpd[p];
+  target_self_kernel<D, CT, DT><<<nblk, 256, 0, c.stream>>>(c.tgt64 + (size_t)P.tg_off * 8, P.Et,
+                                                            cw, dw, part);
+  return cudaGetLastError();
+}
+
+template <int D>
+static bool pick_def(int order, lddmm_ctx &c) {
+  switch (order) {
+    case -1: c.shoot = shoot_impl<D, -1>; c.adjoint = adjoint_impl<D, -1>; return true;
+    case 0: if (D == 3) { c.shoot = shoot_impl<D, 0>; c.adjoint = adjoint_impl<D, 0>; return true; } break;
+    case 1: if (D == 3) { c.shoot = shoot_impl<D, 1>; c.adjoint = adjoint_impl<D, 1>; return true; } break;
+    case 2: if (D == 3) { c.shoot = shoot_impl<D, 2>; c.adjoint = adjoint_impl<D, 2>; return true; } break;
+    case 3: if (D == 3) { c.shoot = shoot_impl<D, 3>; c.adjoint = adjoint_impl<D, 3>; return true; } break;
+    case 4: if (D == 3) { c.shoot = shoot_impl<D, 4>; c.adjoint = adjoint_impl<D, 4>; return true; } break;
+  }
+  return false;
+}
+
+template <int D, char CT>
+static bool pick_vfd_dt(char dt, lddmm_ctx &c) {
+  switch (dt) {
+    case 'B': c.varifold = varifold_impl<D, CT, 'B'>; c.tt = tt_impl<D, CT, 'B'>; return true;
+    case 'L': c.varifold = varifold_impl<D, CT, 'L'>; c.tt = tt_impl<D, CT, 'L'>; return true;
+    case 'O': c.varifold = varifold_impl<D, CT, 'O'>; c.tt = tt_impl<D, CT, 'O'>; return true;
+    case 'U': c.varifold = varifold_impl<D, CT, 'U'>; c.tt = tt_impl<D, CT, 'U'>; return true;
+  }
+  return false;
+}
+
+template <int D>
+static bool pick_vfd(char ct, char dt, lddmm_ctx &c) {
+  if (ct == 'G') return pick_vfd_dt<D, 'G'>(dt, c);
+  if (ct == 'C') return pick_vfd_dt<D, 'C'>(dt, c);
+  return false;
+}
+
+// FP64 alpha (variable layout) -> FP32 point layout used by the sweeps.
+__global__ void alpha_to_f32_kernel(const PairDesc *__restrict__ pd, int P, const double *x,
+                                    float4 *as, int NPtot, int D, int T) {
+  const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  // locate the pair (P is small; linear scan)
+  int p = 0;
+  while (p + 1 < P && v >= pd[p + 1].var_off) ++p;
+  const PairDesc &Q = pd[p];
+  if (v >= Q.var_off + Q.var_num) return;
+  const long long w = v - Q.var_off;
+  const long long nd = (long long)Q.N * D;
+  const int t = (int)(w / nd);
+  const long long rem = w - (long long)t * nd;
+  const int i = (int)(rem / D), d = (int)(rem - (long long)i * D);
+  if (t >= T) return;
+  reinterpret_cast<float *>(as)[((size_t)t * NPtot + Q.pt_off + i) * 4 + d] = (float)x[v];
+}
+
+__global__ void set_int_kernel(int *a, int n, int v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
+// ==================================================================== setup
+
+static int validate(const lddmm_problem &p) {
+  if (p.dim != 2 && p.dim != 3) { set_err("dim must be 2 or 3"); return LDDMM_ERR_ARG; }
+  if (p.nde_num <= 0 || !p.ini_nde) { set_err("nde_num must be positive"); return LDDMM_ERR_ARG; }
+  if (p.time_num < 2) { set_err("time_num must be >= 2"); return LDDMM_ERR_ARG; }
+  if (!(p.knl_width > 0)) { set_err("knl_width must be positive"); return LDDMM_ERR_ARG; }
+  if (p.knl_order < -1 || p.knl_order > 4) { set_err("knl_order must be -1..4"); return LDDMM_ERR_ARG; }
+  if (p.dfm_elm_num < 0 || p.tgt_elm_num < 0) { set_err("negative element count"); return LDDMM_ERR_ARG; }
+  if (p.dfm_elm_num > 0 && !p.dfm_elm_vtx) { set_err("dfm_elm_vtx missing"); return LDDMM_ERR_ARG; }
+  if (p.tgt_elm_num > 0 && (!p.tgt_cen_pos || !p.tgt_uni_dir || !p.tgt_elm_vol)) {
+    set_err("target arrays missing");
+    return LDDMM_ERR_ARG;
+  }
+  if (p.dfm_elm_num > 0 || p.tgt_elm_num > 0) {
+    if (p.cen_knl_type != 'G' && p.cen_knl_type != 'C') { set_err("cen_knl_type must be 'G' or 'C'"); return LDDMM_ERR_ARG; }
+    if (p.dir_knl_type != 'B' && p.dir_knl_type != 'L' && p.dir_knl_type != 'O' && p.dir_knl_type != 'U') {
+      set_err("dir_knl_type must be 'B', 'L', 'O' or 'U'");
+      return LDDMM_ERR_ARG;
+    }
+    if (!(p.cen_knl_width > 0)) { set_err("cen_knl_width must be positive"); return LDDMM_ERR_ARG; }
+    if ((p.dir_knl_type == 'O' || p.dir_knl_type == 'U') && !(p.dir_knl_width > 0)) {
+      set_err("dir_knl_width must be positive for 'O'/'U'");
+      return LDDMM_ERR_ARG;
+    }
+  }
+  for (int e = 0; e < p.dfm_elm_num * p.dim; ++e)
+    if (p.dfm_elm_vtx[e] < 0 || p.dfm_elm_vtx[e] >= p.nde_num) {
+      set_err("dfm_elm_vtx entry %d out of range", e);
+      return LDDMM_ERR_ARG;
+    }
+  return 0;
+}
+
+extern "C" int lddmm_elm_ifo(const int *elm_vtx, int vpe, int elm_num, int nde_num, int *ifo) {
+  // getElmIfo.m:1-59 -- per vertex, adjacent elements in increasing element order
+  // with (2D) sign -1 for the element's first vertex, +1 otherwise, or (3D) the
+  // element's other two vertices (3,2), (1,3), (2,1) for local vertex 1, 2, 3.
+  if ((vpe != 2 && vpe != 3) || elm_num < 0 || nde_num <= 0 || (elm_num > 0 && !elm_vtx)) {
+    set_err("lddmm_elm_ifo: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  std::vector<int> cnt(nde_num, 0);
+  for (int e = 0; e < elm_num * vpe; ++e) {
+    const int v = elm_vtx[e];
+    if (v < 0 || v >= nde_num) {
+      set_err("lddmm_elm_ifo: vertex index out of range");
+      return LDDMM_ERR_ARG;
+    }
+    cnt[v]++;
+  }
+  int mx = 0;
+  for (int v = 0; v < nde_num; ++v) mx = std::max(mx, cnt[v]);
+  const int rows = 1 + mx * vpe;
+  if (!ifo) return rows;
+  std::memset(ifo, 0, sizeof(int) * (size_t)rows * nde_num);
+  static const int other3[3][2] = {{2, 1}, {0, 2}, {1, 0}};
+  for (int e = 0; e < elm_num; ++e)
+    for (int k = 0; k < vpe; ++k) {
+      const int *ev = elm_vtx + (size_t)e * vpe;
+      int *col = ifo + (size_t)ev[k] * rows;
+      const int a = col[0]++;
+      if (vpe == 2) {
+        col[1 + 2 * a] = e;
+        col[2 + 2 * a] = (k == 0) ? -1 : 1;
+      } else {
+        col[1 + 3 * a] = e;
+        col[2 + 3 * a] = ev[other3[k][0]];
+        col[3 + 3 * a] = ev[other3[k][1]];
+      }
+    }
+  return rows;
+}
+
+static int default_cluster(int n_items) {
+  // aim for >= ~4 CTAs per SM of 148 SMs
+  int S = 1;
+  while (S < 8 && n_items * S < 600) S *= 2;
+  return S;
+}
+
+static cudaError_t run_eval(lddmm_ctx &c, double *g_out, double *f_out, double *vlc,
+                            bool grad);
+
+static int autotune(lddmm_ctx &c);
+
+extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm_config *cfg,
+                                lddmm_ctx **out) {
+  if (!out || !probs || num <= 0) {
+    set_err("lddmm_ctx_create: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  *out = nullptr;
+  for (int p = 0; p < num; ++p) {
+    const int rc = validate(probs[p]);
+    if (rc) return rc;
+    const lddmm_problem &a = probs[p], &b = probs[0];
+    if (a.dim != b.dim || a.time_num != b.time_num || a.knl_order != b.knl_order ||
+        ((a.dfm_elm_num > 0) != (b.dfm_elm_num > 0)) ||
+        (a.dfm_elm_num > 0 && (a.cen_knl_type != b.cen_knl_type || a.dir_knl_type != b.dir_knl_type ||
+                               a.dir_knl_width != b.dir_knl_width))) {
+      set_err("pairs of one batch must share dim, time_num, knl_order and varifold kernel types");
+      return LDDMM_ERR_ARG;
+    }
+  }
+  lddmm_config cf = {};
+  if (cfg) cf = *cfg;
+  std::unique_ptr<lddmm_ctx> cp(new lddmm_ctx());
+  lddmm_ctx &c = *cp;
+  const lddmm_problem &p0 = probs[0];
+  c.D = p0.dim;
+  c.order = p0.knl_order;
+  c.time_num = p0.time_num;
+  c.T = p0.time_num - 1;
+  c.P = num;
+  c.has_vfd = p0.dfm_elm_num > 0;
+  c.ct = c.has_vfd ? p0.cen_knl_type : 'G';
+  c.dt = c.has_vfd ? p0.dir_knl_type : 'B';
+  c.ow2 = (c.dt == 'O' || c.dt == 'U') ? (float)(2.0 / (p0.dir_knl_width * p0.dir_knl_width)) : 0.0f;
+  c.device = cf.device;
+  c.use_graph = (cf.use_graph >= 0);
+  CU(cudaSetDevice(c.device));
+
+  bool ok = (c.D == 3) ? pick_def<3>(c.order, c) : pick_def<2>(c.order, c);
+  if (!ok) {
+    set_err("deformation kernel order %d in %dD is not supported by this build", c.order, c.D);
+    return LDDMM_ERR_UNSUPPORTED;
+  }
+  ok = (c.D == 3) ? pick_vfd<3>(c.ct, c.dt, c) : pick_vfd<2>(c.ct, c.dt, c);
+  if (!ok) {
+    set_err("varifold kernel types not supported");
+    return LDDMM_ERR_UNSUPPORTED;
+  }
+
+  // ---- layout
+  const int D = c.D;
+  c.hpd.resize(num);
+  long long voff = 0;
+  int pt = 0, el = 0, tg = 0, it = 0, et = 0, ch = 0;
+  for (int p = 0; p < num; ++p) {
+    const lddmm_problem &a = probs[p];
+    PairDesc &P = c.hpd[p];
+    std::memset(&P, 0, sizeof(P));
+    P.N = a.nde_num;
+    P.Npad = pad_to(a.nde_num, kTile);
+    P.Ed = a.dfm_elm_num;
+    P.Edpad = pad_to(a.dfm_elm_num, kTile);
+    P.Et = a.tgt_elm_num;
+    P.Etpad = pad_to(a.tgt_elm_num, kTile);
+    P.pt_off = pt;
+    P.el_off = el;
+    P.tg_off = tg;
+    P.itile_off = it;
+    P.etile_off = et;
+    P.var_off = voff;
+    P.var_num = (long long)D * a.nde_num * c.T;
+    P.chunk_off = ch;
+    P.nchunk = (int)((P.var_num + kChunk - 1) / kChunk);
+    P.dt = a.time_stp;
+    P.dis_wgt = a.dis_wgt;
+    def_kernel_scales(a.knl_order, a.knl_width, &P.kscale, &P.pd_fac);
+    if (c.has_vfd) cen_kernel_scales(a.cen_knl_type, a.cen_knl_width, &P.cscale, &P.dc_fac);
+    pt += P.Npad;
+    el += P.Edpad;
+    tg += P.Etpad;
+    it += P.Npad / kTile;
+    et += P.Edpad / kTile;
+    voff += P.var_num;
+    ch += P.nchunk;
+  }
+  c.NPtot = pt;
+  c.EDtot = el;
+  c.ETtot = tg;
+  c.ntile_tot = it;
+  c.netile_tot = et;
+  c.nvar = voff;
+  c.nchunk_tot = ch;
+
+  // work items, largest pairs first (the block scheduler then runs longest first)
+  std::vector<int> order(num);
+  for (int p = 0; p < num; ++p) order[p] = p;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return c.hpd[a].Npad > c.hpd[b].Npad; });
+  std::vector<int2> pti, eli;
+  for (int p : order)
+    for (int k = 0; k < c.hpd[p].Npad / kTile; ++k) pti.push_back(make_int2(p, k));
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return c.hpd[a].Edpad + c.hpd[a].Etpad > c.hpd[b].Edpad + c.hpd[b].Etpad;
+  });
+  for (int p : order)
+    for (int k = 0; k < c.hpd[p].Edpad / kTile; ++k) eli.push_back(make_int2(p, k));
+  c.n_pt_items = (int)pti.size();
+  c.n_el_items = (int)eli.size();
+
+  // host-side arrays
+  std::vector<float4> h_qs(c.NPtot, make_float4(0, 0, 0, 0));
+  std::vector<double> h_q64((size_t)c.NPtot * D, 0.0);
+  std::vector<int> h_ptpair(c.NPtot, -1);
+  std::vector<int4> h_elm(std::max(c.EDtot, 1), make_int4(0, 0, 0, -1));
+  std::vector<float4> h_tc(std::max(c.ETtot, 1), make_float4(0, 0, 0, 0)), h_tn(h_tc);
+  std::vector<double> h_tgt64((size_t)std::max(c.ETtot, 1) * 8, 0.0);
+  std::vector<int> h_adjptr(c.NPtot + 1, 0);
+  std::vector<int4> h_adj;
+  std::vector<int> h_chunk(c.nchunk_tot);
+  for (int p = 0; p < num; ++p) {
+    const lddmm_problem &a = probs[p];
+    const PairDesc &P = c.hpd[p];
+    for (int k = 0; k < P.nchunk; ++k) h_chunk[P.chunk_off + k] = p;
+    for (int i = 0; i < P.N; ++i) {
+      const int g = P.pt_off + i;
+      h_ptpair[g] = p;
+      double q[3] = {0, 0, 0};
+      for (int d = 0; d < D; ++d) q[d] = a.ini_nde[(size_t)i * D + d];
+      for (int d = 0; d < D; ++d) h_q64[(size_t)g * D + d] = q[d];
+      h_qs[g] = make_float4((float)(q[0] * P.kscale), (float)(q[1] * P.kscale),
+                            (float)(q[2] * P.kscale), 0.0f);
+    }
+    for (int e = 0; e < P.Ed; ++e) {
+      const int *v = a.dfm_elm_vtx + (size_t)e * D;
+      h_elm[P.el_off + e] = make_int4(P.pt_off + v[0], P.pt_off + v[1],
+                                      D == 3 ? P.pt_off + v[2] : 0, p);
+    }
+    for (int e = 0; e < P.Et; ++e) {
+      const int g = P.tg_off + e;
+      double cc[3] = {0, 0, 0}, nn[3] = {0, 0, 0};
+      for (int d = 0; d < D; ++d) {
+        cc[d] = a.tgt_cen_pos[(size_t)e * D + d];
+        nn[d] = a.tgt_uni_dir[(size_t)e * D + d];
+      }
+      const double vol = a.tgt_elm_vol[e];
+      h_tc[g] = make_float4((float)(cc[0] * P.cscale), (float)(cc[1] * P.cscale),
+                            (float)(cc[2] * P.cscale), (float)(-vol));
+      h_tn[g] = make_float4((float)nn[0], (float)nn[1], (float)nn[2], 0.0f);
+      double *t8 = &h_tgt64[(size_t)g * 8];
+      for (int d = 0; d < 3; ++d) {
+        t8[d] = cc[d];
+        t8[3 + d] = nn[d];
+      }
+      t8[6] = vol;
+    }
+    // adjacency (given table, or computed like getElmIfo)
+    std::vector<int> ifo;
+    int rows = a.dfm_elm_ifo_num;
+    const int *tab = a.dfm_elm_ifo;
+    if (P.Ed > 0 && (!tab || rows <= 0)) {
+      rows = lddmm_elm_ifo(a.dfm_elm_vtx, D, P.Ed, P.N, nullptr);
+      if (rows < 0) return rows;
+      ifo.resize((size_t)rows * P.N);
+      lddmm_elm_ifo(a.dfm_elm_vtx, D, P.Ed, P.N, ifo.data());
+      tab = ifo.data();
+    }
+    for (int i = 0; i < P.N && P.Ed > 0; ++i) {
+      const int *col = tab + (size_t)i * rows;
+      const int cnt = col[0];
+      if (cnt < 0 || 1 + cnt * D > rows) {
+        set_err("dfm_elm_ifo column %d inconsistent", i);
+        return LDDMM_ERR_ARG;
+      }
+      for (int k = 0; k < cnt; ++k) {
+        const int e = col[1 + D * k];
+        if (e < 0 || e >= P.Ed) {
+          set_err("dfm_elm_ifo element index out of range");
+          return LDDMM_ERR_ARG;
+        }
+        if (D == 3) {
+          const int va = col[2 + 3 * k], vb = col[3 + 3 * k];
+          if (va < 0 || va >= P.N || vb < 0 || vb >= P.N) {
+            set_err("dfm_elm_ifo vertex index out of range");
+            return LDDMM_ERR_ARG;
+          }
+          h_adj.push_back(make_int4(P.el_off + e, P.pt_off + va, P.pt_off + vb, 0));
+        } else {
+          h_adj.push_back(make_int4(P.el_off + e, col[2 + 2 * k], 0, 0));
+        }
+      }
+      h_adjptr[P.pt_off + i + 1] = (int)h_adj.size();
+    }
+    // padded vertices carry the running count
+    for (int i = P.N; i < P.Npad; ++i) h_adjptr[P.pt_off + i + 1] = (int)h_adj.size();
+    if (P.Ed == 0)
+      for (int i = 0; i < P.N; ++i) h_adjptr[P.pt_off + i + 1] = (int)h_adj.size();
+  }
+
+  // ---- device memory
+  CU(dalloc(&c.pd, num));
+  CU(dalloc(&c.act, num));
+  CU(dalloc(&c.st, num));
+  CU(dalloc(&c.qs, (size_t)(c.T + 1) * c.NPtot));
+  CU(dalloc(&c.as, (size_t)c.T * c.NPtot));
+  CU(dalloc(&c.us, (size_t)2 * c.NPtot));
+  CU(dalloc(&c.ls, (size_t)2 * c.NPtot));
+  CU(dalloc(&c.q64, (size_t)(c.T + 1) * c.NPtot * D));
+  CU(dalloc(&c.p64, (size_t)c.NPtot * D));
+  CU(dalloc(&c.ec, std::max(c.EDtot, 1)));
+  CU(dalloc(&c.en, std::max(c.EDtot, 1)));
+  CU(dalloc(&c.tc, std::max(c.ETtot, 1)));
+  CU(dalloc(&c.tn, std::max(c.ETtot, 1)));
+  CU(dalloc(&c.e64, (size_t)std::max(c.EDtot, 1) * 4));
+  CU(dalloc(&c.dcdd, (size_t)std::max(c.EDtot, 1) * 2 * D));
+  CU(dalloc(&c.tgt64, h_tgt64.size()));
+  CU(dalloc(&c.elm, h_elm.size()));
+  CU(dalloc(&c.pt_pair, c.NPtot));
+  CU(dalloc(&c.adj_ptr, c.NPtot + 1));
+  CU(dalloc(&c.adj, std::max<size_t>(h_adj.size(), 1)));
+  CU(dalloc(&c.reg_part, (size_t)c.T * c.ntile_tot));
+  CU(dalloc(&c.vfd_part, std::max(c.netile_tot, 1)));
+  CU(dalloc(&c.f_dev, num));
+  CU(dalloc(&c.pt_items, std::max(c.n_pt_items, 1)));
+  CU(dalloc(&c.el_items, std::max(c.n_el_items, 1)));
+  CU(dalloc(&c.chunk_pair, c.nchunk_tot));
+  CU(dalloc(&c.XT, c.nvar));
+  CU(dalloc(&c.GT, c.nvar));
+  CU(dalloc(&c.part[0], (size_t)c.nchunk_tot * 3));
+  CU(dalloc(&c.part[1], (size_t)c.nchunk_tot * 3));
+
+  CU(cudaMemcpy(c.qs, h_qs.data(), sizeof(float4) * c.NPtot, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(c.q64, h_q64.data(), sizeof(double) * h_q64.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(c.pt_pair, h_ptpair.data(), sizeof(int) * c.NPtot, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(c.elm, h_elm.data(), sizeof(int4) * h_elm.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(c.tc, h_tc.data(), sizeof(float4) * h_tc.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(c.tn, h_tn.data(), sizeof(float4) * h_tn.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(c.tgt64, h_tgt64.data(), sizeof(double) * h_tgt64.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(c.adj_ptr, h_adjptr.data(), sizeof(int) * h_adjptr.size(), cudaMemcpyHostToDevice));
+  if (!h_adj.empty())
+    CU(cudaMemcpy(c.adj, h_adj.data(), sizeof(int4) * h_adj.size(), cudaMemcpyHostToDevice));
+  if (c.n_pt_items)
+    CU(cudaMemcpy(c.pt_items, pti.data(), sizeof(int2) * pti.size(), cudaMemcpyHostToDevice));
+  if (c.n_el_items)
+    CU(cudaMemcpy(c.el_items, eli.data(), sizeof(int2) * eli.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(c.chunk_pair, h_chunk.data(), sizeof(int) * h_chunk.size(), cudaMemcpyHostToDevice));
+
+  if (cf.stream) {
+    c.stream = (cudaStream_t)cf.stream;
+  } else {
+    CU(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+    c.own_stream = true;
+  }
+
+  // ---- target self-term, FP64, once
+  for (int p = 0; p < num && c.has_vfd; ++p) {
+    const PairDesc &P = c.hpd[p];
+    if (P.Et == 0) continue;
+    const int nblk = (P.Et + 255) / 256;
+    double *part = nullptr;
+    CU(dalloc(&part, nblk));
+    const double dw = probs[p].dir_knl_width > 0 ? probs[p].dir_knl_width : 1.0;
+    cudaError_t e = c.tt(c, p, part, nblk, probs[p].cen_knl_width, dw);
+    std::vector<double> hp(nblk);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hp.data(), part, sizeof(double) * nblk,
+                                              cudaMemcpyDeviceToHost, c.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+    cudaFree(part);
+    CU(e);
+    double tt = 0.0;
+    for (double x : hp) tt += x;
+    c.hpd[p].tt = tt;
+  }
+  CU(cudaMemcpy(c.pd, c.hpd.data(), sizeof(PairDesc) * num, cudaMemcpyHostToDevice));
+
+  c.S_shoot = cf.cluster_shoot > 0 ? cf.cluster_shoot : default_cluster(c.n_pt_items);
+  c.S_adj = cf.cluster_adjoint > 0 ? cf.cluster_adjoint : default_cluster(c.n_pt_items);
+  c.S_vfd = cf.cluster_varifold > 0 ? cf.cluster_varifold : default_cluster(c.n_el_items);
+  for (int *s : {&c.S_shoot, &c.S_adj, &c.S_vfd})
+    if (*s != 1 && *s != 2 && *s != 4 && *s != 8) {
+      set_err("cluster sizes must be 1, 2, 4 or 8");
+      return LDDMM_ERR_ARG;
+    }
+  if (cf.autotune) {
+    const int rc = autotune(c);
+    if (rc) return rc;
+  }
+  *out = cp.release();
+  return 0;
+}
+
+extern "C" void lddmm_ctx_destroy(lddmm_ctx *ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  delete ctx;
+}
+
+extern "C" int lddmm_ctx_num_pairs(const lddmm_ctx *c) { return c ? c->P : 0; }
+extern "C" long long lddmm_ctx_var_num(const lddmm_ctx *c, int p) {
+  return (c && p >= 0 && p < c->P) ? c->hpd[p].var_num : -1;
+}
+extern "C" long long lddmm_ctx_var_offset(const lddmm_ctx *c, int p) {
+  return (c && p >= 0 && p < c->P) ? c->hpd[p].var_off : -1;
+}
+extern "C" long long lddmm_ctx_var_total(const lddmm_ctx *c) { return c ? c->nvar : -1; }
+extern "C" void *lddmm_ctx_stream(const lddmm_ctx *c) { return c ? (void *)c->stream : nullptr; }
+extern "C" int lddmm_ctx_launch_config(const lddmm_ctx *c, int *o) {
+  if (!c || !o) return LDDMM_ERR_ARG;
+  o[0] = c->S_shoot;
+  o[1] = c->S_adj;
+  o[2] = c->S_vfd;
+  return 0;
+}
+
+// ================================================================ objective
+
+// One objective (and gradient) evaluation of every active pair at XT / as.
+static cudaError_t run_eval(lddmm_ctx &c, double *g_out, double *f_out, double *vlc,
+                            bool grad) {
+  const int D = c.D;
+  for (int t = 0; t < c.T; ++t)
+    CUE(c.shoot(c, t, vlc ? vlc + (size_t)t * c.NPtot * D : nullptr));
+  const double *q64T = c.q64 + (size_t)c.T * c.NPtot * D;
+  if (c.has_vfd) {
+    const int nb = (c.EDtot + 127) / 128;
+    if (D == 3)
+      geometry_kernel<3><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
+    else
+      geometry_kernel<2><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
+    CUE(cudaGetLastError());
+    CUE(c.varifold(c));
+  }
+  if (grad) {
+    const int nb = (c.NPtot + 127) / 128;
+    float4 *un = c.us + (size_t)((c.T - 1) & 1) * c.NPtot;
+    float4 *ln = c.ls + (size_t)((c.T - 1) & 1) * c.NPtot;
+    if (D == 3)
+      gather_kernel<3><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
+                                                  c.dcdd, q64T, c.XT, c.p64, un, ln, nullptr, c.T);
+    else
+      gather_kernel<2><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
+                                                  c.dcdd, q64T, c.XT, c.p64, un, ln, nullptr, c.T);
+    CUE(cudaGetLastError());
+  }
+  objective_kernel<<<c.P, 128, 0, c.stream>>>(c.pd, c.act, c.reg_part, c.ntile_tot, c.vfd_part,
+                                               c.T, c.st, f_out);
+  CUE(cudaGetLastError());
+  if (grad)
+    for (int t = c.T - 1; t >= 0; --t) CUE(c.adjoint(c, t, g_out, nullptr));
+  return cudaSuccess;
+}
+
+static cudaError_t load_trial(lddmm_ctx &c, const double *d_alp, bool host) {
+  CUE(cudaMemcpyAsync(c.XT, d_alp, sizeof(double) * c.nvar,
+                      host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c.stream));
+  const long long n = c.nvar;
+  alpha_to_f32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(c.pd, c.P, c.XT, c.as,
+                                                                          c.NPtot, c.D, c.T);
+  return cudaGetLastError();
+}
+
+extern "C" int lddmm_objgrd_device(lddmm_ctx *ctx, const double *d_alp, double *d_fcn,
+                                   double *d_grd, int async) {
+  if (!ctx || !d_alp || !d_fcn) {
+    set_err("lddmm_objgrd_device: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  lddmm_ctx &c = *ctx;
+  CU(cudaSetDevice(c.device));
+  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
+  CU(cudaGetLastError());
+  CU(load_trial(c, d_alp, false));
+  CU(run_eval(c, d_grd ? d_grd : c.GT, d_fcn, nullptr, true));
+  if (!async) CU(cudaStreamSynchronize(c.stream));
+  return 0;
+}
+
+extern "C" int lddmm_objgrd(lddmm_ctx *ctx, const double *alp, double *fcn, double *grd) {
+  if (!ctx || !alp || !fcn) {
+    set_err("lddmm_objgrd: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  lddmm_ctx &c = *ctx;
+  CU(cudaSetDevice(c.device));
+  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
+  CU(cudaGetLastError());
+  CU(load_trial(c, alp, true));
+  CU(run_eval(c, c.GT, c.f_dev, nullptr, grd != nullptr));
+  CU(cudaMemcpyAsync(fcn, c.f_dev, sizeof(double) * c.P, cudaMemcpyDeviceToHost, c.stream));
+  if (grd) CU(cudaMemcpyAsync(grd, c.GT, sizeof(double) * c.nvar, cudaMemcpyDeviceToHost, c.stream));
+  CU(cudaStreamSynchronize(c.stream));
+  return 0;
+}
+
+extern "C" int lddmm_shoot(lddmm_ctx *ctx, const double *alp, double *nde_stk, double *vlc_stk) {
+  if (!ctx || !alp) {
+    set_err("lddmm_shoot: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  lddmm_ctx &c = *ctx;
+  const int D = c.D;
+  CU(cudaSetDevice(c.device));
+  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
+  CU(load_trial(c, alp, true));
+  double *vlc = nullptr;
+  CU(dalloc(&vlc, (size_t)c.T * c.NPtot * D));
+  cudaError_t e = cudaSuccess;
+  for (int t = 0; t < c.T && e == cudaSuccess; ++t)
+    e = c.shoot(c, t, vlc + (size_t)t * c.NPtot * D);
+  std::vector<double> hq((size_t)(c.T + 1) * c.NPtot * D), hv((size_t)c.T * c.NPtot * D);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hq.data(), c.q64, sizeof(double) * hq.size(), cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hv.data(), vlc, sizeof(double) * hv.size(), cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+  cudaFree(vlc);
+  CU(e);
+  // un-pad: per pair, time-major blocks of N x D
+  size_t on = 0, ov = 0;
+  for (int p = 0; p < c.P; ++p) {
+    const PairDesc &P = c.hpd[p];
+    for (int t = 0; t <= c.T; ++t)
+      for (int i = 0; i < P.N; ++i)
+        for (int d = 0; d < D; ++d) {
+          const size_t src = ((size_t)t * c.NPtot + P.pt_off + i) * D + d;
+          if (nde_stk) nde_stk[on] = hq[src];
+          ++on;
+          if (t < c.T) {
+            if (vlc_stk) vlc_stk[ov] = hv[src];
+            ++ov;
+          }
+        }
+  }
+  return 0;
+}
+
+// ==================================================================== L-BFGS
+
+static cudaError_t ensure_lbfgs_buffers(lddmm_ctx &c, int m, int rec_cap) {
+  if (!c.X) {
+    CUE(dalloc(&c.X, c.nvar));
+    CUE(dalloc(&c.G, c.nvar));
+    CUE(dalloc(&c.Dv, c.nvar));
+    CUE(dalloc(&c.Qv, c.nvar));
+  }
+  if (c.m_alloc < m) {
+    dfree(c.Sh);
+    dfree(c.Yh);
+    CUE(dalloc(&c.Sh, (size_t)m * c.nvar));
+    CUE(dalloc(&c.Yh, (size_t)m * c.nvar));
+    c.m_alloc = m;
+    c.graph_valid = false;
+  }
+  if (c.rec_cap < rec_cap) {
+    dfree(c.rec);
+    CUE(dalloc(&c.rec, (size_t)c.P * rec_cap * 4));
+    c.rec_cap = rec_cap;
+    c.graph_valid = false;
+  }
+  return cudaSuccess;
+}
+
+static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o) {
+  CUE(run_eval(c, c.GT, nullptr, nullptr, true));
+  VecArgs A;
+  A.pd = c.pd;
+  A.st = c.st;
+  A.chunk_pair = c.chunk_pair;
+  A.X = c.X; A.G = c.G; A.XT = c.XT; A.GT = c.GT; A.Dv = c.Dv; A.Qv = c.Qv;
+  A.S = c.Sh; A.Y = c.Yh;
+  A.nvar = c.nvar;
+  A.as = c.as;
+  A.NPtot = c.NPtot;
+  A.D = c.D;
+  A.m = o.mem_num;
+  const unsigned nb = (unsigned)c.nchunk_tot;
+  const int pb = (c.P + 127) / 128;
+  int s = 0;  // pass sequence number: writes part[s & 1], reads part[(s - 1) & 1]
+  auto pass = [&](int mode, int k) -> cudaError_t {
+    A.part_out = c.part[s & 1];
+    A.part_in = c.part[(s + 1) & 1];
+    vec_pass_kernel<<<nb, kVecThreads, 0, c.stream>>>(A, mode, k);
+    ++s;
+    return cudaGetLastError();
+  };
+  CUE(pass(kPost, 0));
+  decide_kernel<<<pb, 128, 0, c.stream>>>(c.pd, c.st, c.P, c.part[0], o, c.rec);
+  CUE(cudaGetLastError());
+  CUE(pass(kAccept, 0));
+  for (int k = 0; k < o.mem_num; ++k) CUE(pass(kTwoLoopB, k));
+  for (int k = 0; k < o.mem_num; ++k) CUE(pass(kTwoLoopF, k));
+  CUE(pass(kFin, 0));
+  ls_init_kernel<<<pb, 128, 0, c.stream>>>(c.pd, c.st, c.P, c.part[(s - 1) & 1], c.act);
+  return cudaGetLastError();
+}
+
+static long long kernels_per_cycle(const lddmm_ctx &c, int m) {
+  // objective: T shooting + [geometry + varifold] + gather + objective + T adjoint;
+  // optimiser: POST, DECIDE, ACCEPT, m + m two-loop passes, FIN, LSINIT
+  return 2LL * c.T + 2 + (c.has_vfd ? 2 : 0) + 2LL * m + 5;
+}
+
+static bool same_opt(const OptParams &a, const OptParams &b) {
+  return std::memcmp(&a, &b, sizeof(OptParams)) == 0;
+}
+
+static int build_graph(lddmm_ctx &c, const OptParams &o) {
+  if (c.graph_valid && same_opt(c.graph_opt, o)) return 0;
+  if (c.cycle_exec) {
+    cudaGraphExecDestroy(c.cycle_exec);
+    c.cycle_exec = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CU(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = launch_cycle(c, o);
+  cudaError_t e2 = cudaStreamEndCapture(c.stream, &g);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    CU(e != cudaSuccess ? e : e2);
+  }
+  e = cudaGraphInstantiate(&c.cycle_exec, g, 0);
+  cudaGraphDestroy(g);
+  CU(e);
+  c.graph_opt = o;
+  c.graph_valid = true;
+  return 0;
+}
+
+static void print_table(const lddmm_ctx &c, int p, const std::vector<double> &rec, int rows) {
+  // the reference's verbose table (Cpp/src/LBFGS.cpp:54-61, 107-108)
+  if (c.P > 1) printf("pair %d\n", p);
+  printf("%5s   %13s  %13s  %13s  %9s\n", "iter", "f", "|grad f|", "step length", "fcn eval");
+  char sep[65] = {0};
+  std::memset(sep, '-', 62);
+  printf("%s\n", sep);
+  for (int k = 0; k < rows; ++k) {
+    const double *r = &rec[((size_t)p * c.rec_cap + k) * 4];
+    if (k == 0)
+      printf("%5d:  %13.6e  %13.6e\n", 0, r[0], r[1]);
+    else
+      printf("%5d:  %13.6e  %13.6e  %13.6e  %9d\n", k, r[0], r[1], r[2], (int)r[3]);
+  }
+  fflush(stdout);
+}
+
+static int lbfgs_run(lddmm_ctx &c, const lddmm_opt *opt, const double *alp, bool host,
+                     double *alp_out, lddmm_result *res) {
+  if (!opt || opt->mem_num < 1 || opt->mem_num > kMaxMem || opt->itr_max < 0 || !(opt->tol_val >= 0)) {
+    set_err("lddmm_lbfgs: bad options (mem_num must be 1..%d)", kMaxMem);
+    return LDDMM_ERR_ARG;
+  }
+  OptParams o;
+  std::memset(&o, 0, sizeof(o));
+  o.itr_max = opt->itr_max;
+  o.mem_num = opt->mem_num;
+  o.tol = opt->tol_val;
+  o.wolfe1 = opt->wolfe1;
+  o.wolfe2 = opt->wolfe2;
+  o.rel_obj_tol = opt->rel_obj_tol;
+  o.rec_cap = std::min(opt->itr_max + 1, 100001);
+  CU(cudaSetDevice(c.device));
+  CU(ensure_lbfgs_buffers(c, o.mem_num, o.rec_cap));
+  // initial state: every pair evaluates its starting point
+  std::vector<PairState> hs(c.P);
+  for (auto &s : hs) {
+    std::memset(&s, 0, sizeof(s));
+    s.phase = kPhaseInit;
+    s.active = 1;
+    s.newIdx = -1;
+  }
+  CU(cudaMemcpyAsync(c.st, hs.data(), sizeof(PairState) * c.P, cudaMemcpyHostToDevice, c.stream));
+  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
+  CU(cudaGetLastError());
+  CU(load_trial(c, alp, host));
+  CU(cudaMemcpyAsync(c.X, c.XT, sizeof(double) * c.nvar, cudaMemcpyDeviceToDevice, c.stream));
+  if (c.use_graph) {
+    const int rc = build_graph(c, o);
+    if (rc) return rc;
+  }
+  // safety bound on cycles: every iteration takes at most bisMax + epdMax + 2
+  // evaluations (>= 62); the per-pair state machine ends well before this.
+  const long long max_cycles = (long long)o.itr_max * 200 + 8;
+  std::vector<int> hact(c.P);
+  long long cycles = 0;
+  const int check_every = 4;
+  bool timed_out = false;
+  while (true) {
+    for (int k = 0; k < check_every; ++k) {
+      if (c.use_graph)
+        CU(cudaGraphLaunch(c.cycle_exec, c.stream));
+      else
+        CU(launch_cycle(c, o));
+    }
+    cycles += check_every;
+    CU(cudaMemcpyAsync(hact.data(), c.act, sizeof(int) * c.P, cudaMemcpyDeviceToHost, c.stream));
+    CU(cudaStreamSynchronize(c.stream));
+    bool any = false;
+    for (int a : hact) any |= (a != 0);
+    if (!any) break;
+    if (cycles >= max_cycles) {
+      timed_out = true;
+      break;
+    }
+  }
+  c.last_cycles = cycles;
+  c.last_launches = cycles * kernels_per_cycle(c, o.mem_num) + 2;
+  CU(cudaMemcpyAsync(hs.data(), c.st, sizeof(PairState) * c.P, cudaMemcpyDeviceToHost, c.stream));
+  CU(cudaMemcpyAsync(alp_out, c.X, sizeof(double) * c.nvar,
+                     host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, c.stream));
+  CU(cudaStreamSynchronize(c.stream));
+  int ret = 0;
+  c.last_evals = 0;
+  for (int p = 0; p < c.P; ++p) c.last_evals += hs[p].evals;
+  for (int p = 0; p < c.P; ++p) {
+    const PairState &s = hs[p];
+    int status = s.status;
+    if (timed_out && (s.phase == kPhaseInit || s.phase == kPhaseLS)) status = LDDMM_ERR_TIMEOUT;
+    if (res) {
+      res[p].fcn = s.f;
+      res[p].grd_len = s.glen;
+      res[p].status = status;
+      res[p].iters = s.iters;
+      res[p].evals = s.evals;
+      res[p].pad_ = 0;
+    }
+    if (status != 0 && ret == 0) ret = status;
+  }
+  if (opt->vbs_flg) {
+    std::vector<double> rec((size_t)c.P * c.rec_cap * 4);
+    CU(cudaMemcpy(rec.data(), c.rec, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost));
+    for (int p = 0; p < c.P; ++p)
+      print_table(c, p, rec, std::min(hs[p].iters + 1, c.rec_cap));
+  }
+  return ret;
+}
+
+extern "C" int lddmm_lbfgs(lddmm_ctx *ctx, const lddmm_opt *opt, double *alp_inout,
+                           lddmm_result *res) {
+  if (!ctx || !alp_inout) {
+    set_err("lddmm_lbfgs: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  return lbfgs_run(*ctx, opt, alp_inout, true, alp_inout, res);
+}
+
+extern "C" int lddmm_lbfgs_device(lddmm_ctx *ctx, const lddmm_opt *opt, double *d_alp_inout,
+                                  lddmm_result *res) {
+  if (!ctx || !d_alp_inout) {
+    set_err("lddmm_lbfgs_device: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  return lbfgs_run(*ctx, opt, d_alp_inout, false, d_alp_inout, res);
+}
+
+extern "C" int lddmm_lbfgs_trace(const lddmm_ctx *ctx, int pair, double *rows4, int cap) {
+  if (!ctx || pair < 0 || pair >= ctx->P || !rows4 || !ctx->rec) return LDDMM_ERR_ARG;
+  PairState s;
+  if (cudaMemcpy(&s, ctx->st + pair, sizeof(s), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return LDDMM_ERR_CUDA;
+  const int n = std::min({s.iters + 1, ctx->rec_cap, cap});
+  if (cudaMemcpy(rows4, ctx->rec + (size_t)pair * ctx->rec_cap * 4, sizeof(double) * 4 * n,
+                 cudaMemcpyDeviceToHost) != cudaSuccess)
+    return LDDMM_ERR_CUDA;
+  return n;
+}
+
+extern "C" int lddmm_ctx_counters(const lddmm_ctx *ctx, long long *out, int n) {
+  if (!ctx || !out || n < 0) return LDDMM_ERR_ARG;
+  const long long v[4] = {ctx->last_cycles, ctx->last_cycles ? ctx->last_launches / ctx->last_cycles : 0,
+                          ctx->last_launches, ctx->last_evals};
+  const int k = std::min(n, 4);
+  for (int i = 0; i < k; ++i) out[i] = v[i];
+  if (k >= 2 && ctx->last_cycles) out[1] = kernels_per_cycle(*ctx, ctx->graph_opt.mem_num);
+  return k;
+}
+
+extern "C" int lddmm_ctx_time_sweeps(lddmm_ctx *ctx, int reps, double *ms4) {
+  if (!ctx || reps <= 0 || !ms4) return LDDMM_ERR_ARG;
+  lddmm_ctx &c = *ctx;
+  CU(cudaSetDevice(c.device));
+  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
+  CU(cudaGetLastError());
+  const int nev = 2 * c.T + 1;
+  std::vector<cudaEvent_t> ev(2 * nev + 2);
+  for (auto &e : ev) CU(cudaEventCreate(&e));
+  double acc[4] = {0, 0, 0, 0};
+  int cnt[3] = {0, 0, 0};
+  const int D = c.D;
+  cudaError_t err = cudaSuccess;
+  for (int r = 0; r < reps && err == cudaSuccess; ++r) {
+    cudaEventRecord(ev[2 * nev], c.stream);
+    for (int t = 0; t < c.T; ++t) {
+      cudaEventRecord(ev[2 * t], c.stream);
+      err = c.shoot(c, t, nullptr);
+      cudaEventRecord(ev[2 * t + 1], c.stream);
+    }
+    const double *q64T = c.q64 + (size_t)c.T * c.NPtot * D;
+    if (c.has_vfd) {
+      const int nb = (c.EDtot + 127) / 128;
+      if (D == 3)
+        geometry_kernel<3><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
+      else
+        geometry_kernel<2><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
+      cudaEventRecord(ev[4 * c.T], c.stream);
+      if (err == cudaSuccess) err = c.varifold(c);
+      cudaEventRecord(ev[4 * c.T + 1], c.stream);
+    }
+    const int nb = (c.NPtot + 127) / 128;
+    float4 *un = c.us + (size_t)((c.T - 1) & 1) * c.NPtot;
+    float4 *ln = c.ls + (size_t)((c.T - 1) & 1) * c.NPtot;
+    if (D == 3)
+      gather_kernel<3><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
+                                                  c.dcdd, q64T, c.XT, c.p64, un, ln, nullptr, c.T);
+    else
+      gather_kernel<2><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
+                                                  c.dcdd, q64T, c.XT, c.p64, un, ln, nullptr, c.T);
+    objective_kernel<<<c.P, 128, 0, c.stream>>>(c.pd, c.act, c.reg_part, c.ntile_tot, c.vfd_part,
+                                                 c.T, nullptr, c.f_dev);
+    for (int t = c.T - 1; t >= 0 && err == cudaSuccess; --t) {
+      cudaEventRecord(ev[2 * c.T + 2 * t], c.stream);
+      err = c.adjoint(c, t, c.GT, nullptr);
+      cudaEventRecord(ev[2 * c.T + 2 * t + 1], c.stream);
+    }
+    cudaEventRecord(ev[2 * nev + 1], c.stream);
+    if (err == cudaSuccess) err = cudaEventSynchronize(ev[2 * nev + 1]);
+    if (err != cudaSuccess) break;
+    float ms = 0.0f;
+    for (int t = 0; t < c.T; ++t) {
+      cudaEventElapsedTime(&ms, ev[2 * t], ev[2 * t + 1]);
+      acc[0] += ms;
+      cnt[0]++;
+      cudaEventElapsedTime(&ms, ev[2 * c.T + 2 * t], ev[2 * c.T + 2 * t + 1]);
+      acc[1] += ms;
+      cnt[1]++;
+    }
+    if (c.has_vfd) {
+      cudaEventElapsedTime(&ms, ev[4 * c.T], ev[4 * c.T + 1]);
+      acc[2] += ms;
+      cnt[2]++;
+    }
+    cudaEventElapsedTime(&ms, ev[2 * nev], ev[2 * nev + 1]);
+    acc[3] += ms;
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  CU(err);
+  ms4[0] = cnt[0] ? acc[0] / cnt[0] : 0.0;
+  ms4[1] = cnt[1] ? acc[1] / cnt[1] : 0.0;
+  ms4[2] = cnt[2] ? acc[2] / cnt[2] : 0.0;
+  ms4[3] = acc[3] / reps;
+  return 0;
+}
+
+// =============================================================== autotuner
+
+static int autotune(lddmm_ctx &c) {
+  // Time every cluster size for each sweep on this batch (zero momenta; the cost
+  // does not depend on the values) and keep the fastest.
+  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
+  CU(cudaGetLastError());
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  const int cands[4] = {1, 2, 4, 8};
+  int *slots[3] = {&c.S_shoot, &c.S_adj, &c.S_vfd};
+  for (int which = 0; which < 3; ++which) {
+    if (which == 2 && !c.has_vfd) break;
+    float best = 1e30f;
+    int bestS = *slots[which];
+    for (int S : cands) {
+      *slots[which] = S;
+      float ms = 0.0f;
+      for (int rep = 0; rep < 4; ++rep) {
+        CU(cudaEventRecord(e0, c.stream));
+        cudaError_t e = (which == 0) ? c.shoot(c, 0, nullptr)
+                        : (which == 1) ? c.adjoint(c, 0, c.GT, nullptr)
+                                       : c.varifold(c);
+        CU(e);
+        CU(cudaEventRecord(e1, c.stream));
+        CU(cudaEventSynchronize(e1));
+        float t = 0.0f;
+        CU(cudaEventElapsedTime(&t, e0, e1));
+        if (rep > 0) ms += t;
+      }
+      if (ms < best) {
+        best = ms;
+        bestS = S;
+      }
+    }
+    *slots[which] = bestS;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // the trial sweeps wrote the step-1 positions and adjoint state; reset them
+  CU(cudaMemsetAsync(c.p64, 0, sizeof(double) * c.NPtot * c.D, c.stream));
+  CU(cudaStreamSynchronize(c.stream));
+  return 0;
+}
+
+// ===================================================== single-call helpers
+
+static lddmm_problem point_problem(int dim, int n, const double *q, int order, double width) {
+  lddmm_problem p;
+  std::memset(&p, 0, sizeof(p));
+  p.dim = dim;
+  p.nde_num = n;
+  p.time_num = 2;
+  p.time_stp = 1.0;
+  p.knl_order = order;
+  p.knl_width = width;
+  p.ini_nde = q;
+  p.dis_wgt = 1.0;
+  p.cen_knl_type = 'G';
+  p.cen_knl_width = 1.0;
+  p.dir_knl_type = 'B';
+  return p;
+}
+
+extern "C" int lddmm_multiply_kernel(int dim, int n, const double *q, const double *a,
+                                     int order, double width, double *v) {
+  if (!q || !a || !v) {
+    set_err("lddmm_multiply_kernel: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  lddmm_problem p = point_problem(dim, n, q, order, width);
+  lddmm_ctx *ctx = nullptr;
+  lddmm_config cfg = {};
+  cfg.use_graph = -1;
+  int rc = lddmm_ctx_create(&p, 1, &cfg, &ctx);
+  if (rc) return rc;
+  std::unique_ptr<lddmm_ctx, void (*)(lddmm_ctx *)> guard(ctx, lddmm_ctx_destroy);
+  std::vector<double> vs((size_t)2 * n * dim), qs;
+  rc = lddmm_shoot(ctx, a, nullptr, vs.data());
+  if (rc) return rc;
+  std::memcpy(v, vs.data(), sizeof(double) * n * dim);
+  return 0;
+}
+
+extern "C" int lddmm_dq_kernel(int dim, int n, const double *q, const double *l, const double *r,
+                               int order, double width, double *dq) {
+  if (!q || !l || !r || !dq) {
+    set_err("lddmm_dq_kernel: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  lddmm_problem p = point_problem(dim, n, q, order, width);
+  lddmm_ctx *ctx = nullptr;
+  lddmm_config cfg = {};
+  cfg.use_graph = -1;
+  int rc = lddmm_ctx_create(&p, 1, &cfg, &ctx);
+  if (rc) return rc;
+  std::unique_ptr<lddmm_ctx, void (*)(lddmm_ctx *)> guard(ctx, lddmm_ctx_destroy);
+  lddmm_ctx &c = *ctx;
+  const PairDesc &P = c.hpd[0];
+  std::vector<float4> hl(c.NPtot, make_float4(0, 0, 0, 0)), hr(hl);
+  for (int i = 0; i < n; ++i) {
+    float a[3] = {0, 0, 0}, b[3] = {0, 0, 0};
+    for (int d = 0; d < dim; ++d) {
+      a[d] = (float)l[(size_t)i * dim + d];
+      b[d] = (float)r[(size_t)i * dim + d];
+    }
+    hl[P.pt_off + i] = make_float4(a[0], a[1], a[2], 0.0f);
+    hr[P.pt_off + i] = make_float4(b[0], b[1], b[2], 0.0f);
+  }
+  double *pd = nullptr;
+  CU(dalloc(&pd, (size_t)c.NPtot * dim));
+  std::unique_ptr<double, cudaError_t (*)(void *)> pguard(pd, cudaFree);
+  CU(cudaMemsetAsync(c.us, 0, sizeof(float4) * c.NPtot, c.stream));
+  CU(cudaMemcpyAsync(c.ls, hl.data(), sizeof(float4) * c.NPtot, cudaMemcpyHostToDevice, c.stream));
+  CU(cudaMemcpyAsync(c.as, hr.data(), sizeof(float4) * c.NPtot, cudaMemcpyHostToDevice, c.stream));
+  set_int_kernel<<<1, 32, 0, c.stream>>>(c.act, 1, 1);
+  CU(c.adjoint(c, 0, nullptr, pd));
+  std::vector<double> h((size_t)c.NPtot * dim);
+  CU(cudaMemcpyAsync(h.data(), pd, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c.stream));
+  CU(cudaStreamSynchronize(c.stream));
+  std::memcpy(dq, h.data() + (size_t)P.pt_off * dim, sizeof(double) * n * dim);
+  return 0;
+}
+
+extern "C" int lddmm_varifold(const lddmm_problem *prob, const double *nde, double *val,
+                              double *dq) {
+  if (!prob || !nde || !val) {
+    set_err("lddmm_varifold: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  lddmm_problem p = *prob;
+  p.ini_nde = nde;
+  p.time_num = 2;
+  p.time_stp = 1.0;
+  if (p.knl_order < -1 || p.knl_order > 4 || (p.dim == 2 && p.knl_order != -1)) p.knl_order = -1;
+  if (!(p.knl_width > 0)) p.knl_width = 1.0;
+  p.dis_wgt = 1.0;
+  lddmm_ctx *ctx = nullptr;
+  lddmm_config cfg = {};
+  cfg.use_graph = -1;
+  int rc = lddmm_ctx_create(&p, 1, &cfg, &ctx);
+  if (rc) return rc;
+  std::unique_ptr<lddmm_ctx, void (*)(lddmm_ctx *)> guard(ctx, lddmm_ctx_destroy);
+  lddmm_ctx &c = *ctx;
+  const int D = c.D;
+  // positions at the final time = nde; zero energy partials
+  double *q64T = c.q64 + (size_t)c.T * c.NPtot * D;
+  CU(cudaMemcpyAsync(q64T, c.q64, sizeof(double) * c.NPtot * D, cudaMemcpyDeviceToDevice, c.stream));
+  CU(cudaMemsetAsync(c.reg_part, 0, sizeof(double) * c.T * c.ntile_tot, c.stream));
+  set_int_kernel<<<1, 32, 0, c.stream>>>(c.act, 1, 1);
+  double *dqd = nullptr;
+  CU(dalloc(&dqd, (size_t)c.NPtot * D));
+  std::unique_ptr<double, cudaError_t (*)(void *)> g2(dqd, cudaFree);
+  if (c.has_vfd) {
+    const int nb = (c.EDtot + 127) / 128;
+    if (D == 3)
+      geometry_kernel<3><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
+    else
+      geometry_kernel<2><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
+    CU(cudaGetLastError());
+    CU(c.varifold(c));
+    const int np = (c.NPtot + 127) / 128;
+    if (D == 3)
+      gather_kernel<3><<<np, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
+                                                  c.dcdd, q64T, c.XT, c.p64, nullptr, nullptr, dqd, c.T);
+    else
+      gather_kernel<2><<<np, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
+                                                  c.dcdd, q64T, c.XT, c.p64, nullptr, nullptr, dqd, c.T);
+    CU(cudaGetLastError());
+  }
+  objective_kernel<<<1, 128, 0, c.stream>>>(c.pd, c.act, c.reg_part, c.ntile_tot, c.vfd_part, c.T,
+                                             nullptr, c.f_dev);
+  CU(cudaGetLastError());
+  std::vector<double> h((size_t)c.NPtot * D);
+  CU(cudaMemcpyAsync(val, c.f_dev, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  CU(cudaMemcpyAsync(h.data(), dqd, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c.stream));
+  CU(cudaStreamSynchronize(c.stream));
+  if (dq) std::memcpy(dq, h.data(), sizeof(double) * (size_t)p.nde_num * D);
+  return 0;
+}
+
+extern "C" int lddmm_LDDMM(int dim, int nde_num, int dfm_elm_num, int dfm_elm_ifo_num,
+                           int tgt_elm_num, const double *iniNdeMat, const double *iniAlpVec,
+                           const int *dfmElmVtxMat, const int *dfmElmIfoMat,
+                           const double *tgtCenPosMat, const double *tgtElmVolVec,
+                           const double *tgtUniDirMat, char cenKnlType, double cenKnlWidth,
+                           char dirKnlType, double dirKnlWidth, double disWgt, int knlOrder,
+                           double knlWidth, double timeStp, int timeNum, int MaxIterations,
+                           double OptimalityTolerance, double Wolfe1, double Wolfe2, int Columns,
+                           int Verbose, double *optAlpVec) {
+  // Cpp/src/LDDMM.cpp:11-98: build the problem, copy the initial momenta, run LBFGS.
+  if (!optAlpVec || !iniAlpVec) {
+    set_err("lddmm_LDDMM: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  lddmm_problem p;
+  std::memset(&p, 0, sizeof(p));
+  p.dim = dim;
+  p.nde_num = nde_num;
+  p.time_num = timeNum;
+  p.time_stp = timeStp;
+  p.knl_order = knlOrder;
+  p.knl_width = knlWidth;
+  p.ini_nde = iniNdeMat;
+  p.dis_wgt = disWgt;
+  p.dfm_elm_num = dfm_elm_num;
+  p.dfm_elm_vtx = dfmElmVtxMat;
+  p.dfm_elm_ifo_num = dfmElmIfoMat ? dfm_elm_ifo_num : 0;
+  p.dfm_elm_ifo = dfmElmIfoMat;
+  p.tgt_elm_num = tgt_elm_num;
+  p.tgt_cen_pos = tgtCenPosMat;
+  p.tgt_uni_dir = tgtUniDirMat;
+  p.tgt_elm_vol = tgtElmVolVec;
+  p.cen_knl_type = cenKnlType;
+  p.cen_knl_width = cenKnlWidth;
+  p.dir_knl_type = dirKnlType;
+  p.dir_knl_width = dirKnlWidth;
+  lddmm_ctx *ctx = nullptr;
+  int rc = lddmm_ctx_create(&p, 1, nullptr, &ctx);
+  if (rc) return rc;
+  std::unique_ptr<lddmm_ctx, void (*)(lddmm_ctx *)> guard(ctx, lddmm_ctx_destroy);
+  const long long n = (long long)dim * nde_num * (timeNum - 1);
+  std::memcpy(optAlpVec, iniAlpVec, sizeof(double) * n);
+  lddmm_opt o;
+  std::memset(&o, 0, sizeof(o));
+  o.itr_max = MaxIterations;
+  o.tol_val = OptimalityTolerance;
+  o.wolfe1 = Wolfe1;
+  o.wolfe2 = Wolfe2;
+  o.mem_num = Columns;
+  o.vbs_flg = Verbose;
+  lddmm_result r;
+  return lddmm_lbfgs(ctx, &o, optAlpVec, &r);
+}
+
+// ============================================================ FP32 probe
+
+// 8 independent FMA chains per thread; the result is stored only under a condition
+// the host never meets, so the compiler keeps every FMA.
+__global__ void fp32_probe_kernel(float *out, int iters, float seed) {
+  float a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = seed + threadIdx.x * 1e-6f + k;
+  const float m = 0.999999f, c = 1e-7f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = fmaf(a[k], m, c);
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += a[k];
+  if (s == -12345.0f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+extern "C" int lddmm_fp32_peak(int device, double *tflops) {
+  if (!tflops) return LDDMM_ERR_ARG;
+  CU(cudaSetDevice(device));
+  int sms = 0;
+  CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  const int threads = 256, blocks = sms * 8, iters = 1 << 15;
+  float *out = nullptr;
+  CU(cudaMalloc(&out, sizeof(float) * threads * blocks));
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; ++rep) {
+    cudaEventRecord(e0);
+    fp32_probe_kernel<<<blocks, threads>>>(out, iters, 1.0f);
+    cudaEventRecord(e1);
+    CU(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0) best = std::min(best, ms);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  *tflops = 2.0 * 8.0 * iters * (double)threads * blocks / (best * 1e-3) / 1e12;
+  return 0;
+}
+
+// ================================================================ misc
+
+extern "C" const char *lddmm_last_error(void) { return g_err.c_str(); }
+extern "C" const char *lddmm_version(void) { return "lddmm_b200 0.1 (sm_100a)"; }
+
+extern "C" double lddmm_flops_per_pair(int sweep, int dim, int order, char ct, char dt) {
+  // Arithmetic executed per pair interaction, FMA = 2 flops, MUFU ops = 1,
+  // compensation overhead (6 flops per accumulator per 32 pairs) not counted.
+  const int D = dim;
+  const double dist = D + 2.0 * D;  // D subtracts, D FMAs for -r2
+  if (sweep == 0) {                 // shooting: K and D FMAs
+    const double k = (order == -1) ? 1.0 : (order == 0 ? 2.0 : (order == 1 ? 5.0 : 5.0 + 2.0 * (order - 1)));
+    return dist + k + 2.0 * D;
+  }
+  if (sweep == 1) {                 // fused adjoint: K, W, lr (2D FMA), s, D + D FMAs
+    const double k = (order == -1) ? 1.0 : (order == 0 ? 2.0 : (order == 1 ? 5.0 : 7.0 + 4.0 * (order - 1)));
+    return dist + k + 2.0 * (2.0 * D) + 1.0 + 2.0 * D + 2.0 * D;
+  }
+  // varifold: centre kernel, ang (D FMAs), kw, direction terms, S, A, C
+  const double cen = (ct == 'G') ? 1.0 : 3.0;
+  double dir = (dt == 'B') ? 3.0 : 6.0;
+  return dist + cen + 2.0 * D + 1.0 + dir + 2.0 * D + 2.0 * D + (ct == 'C' ? 1.0 : 0.0);
+}

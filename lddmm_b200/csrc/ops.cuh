@@ -1,0 +1,499 @@
+// The three all-pairs sweeps of one objective evaluation and the small kernels
+// around them.  Semantics follow Cpp/src/objgrd.cpp:26-90:
+//   forward   v_t = K(q_t) a_t,  E += a_t . v_t,  q_{t+1} = q_t + dt v_t     (:45-59)
+//   varifold  V(q_T), dV/dq_T; E = dt/2 E + w V; p = -w dV/dq                (:61-67)
+//   backward  g_t = dt K(q_t)(a_t - p),
+//             p  <- p - dt dqKernel(q_t, a_t/2 - p, a_t)                      (:69-87)
+// The backward sweep fuses the kernel-matrix product and the dq sum of one step
+// into a single pass over the pairs (they share q_t and the exponential).
+#pragma once
+
+#include "kernels.cuh"
+#include "layout.h"
+#include "sweep.cuh"
+
+namespace lddmm {
+
+// ------------------------------------------------------------------- forward
+
+template <int D, int ORDER>
+struct ShootOp {
+  static constexpr int JW = 2;
+  static constexpr int NA = D;
+  static constexpr bool kTileSum = true;
+  static constexpr bool kTwoSets = false;
+  struct IData {
+    float x, y, z;
+  };
+  const PairDesc *pd;
+  const int *act;
+  const float4 *qs_t;  // scaled positions at t          [NPtot]
+  const float4 *as_t;  // alpha_t (FP32)                 [NPtot]
+  const double *q64_t; // positions at t (FP64)          [NPtot * D]
+  double *q64_n;       // positions at t + 1
+  float4 *qs_n;        // scaled positions at t + 1
+  const double *x64;   // FP64 alpha (trial point), variable layout
+  double *vlc64;       // optional velocity output       [NPtot * D]
+  double *tile_part;   // energy partial per i-tile of this step
+  int t;
+
+  __device__ bool active(int p) const { return act[p] != 0; }
+  __device__ int j_count(int p) const { return pd[p].Npad; }
+  __device__ int j_set(int, int) const { return 0; }
+  __device__ void load_i(int p, int row, IData &I) const {
+    const float4 q = qs_t[pd[p].pt_off + row];
+    I.x = q.x;
+    I.y = q.y;
+    I.z = q.z;
+  }
+  __device__ void load_j(int p, int j, float4 (&w)[JW]) const {
+    const int g = pd[p].pt_off + j;
+    w[0] = __ldg(&qs_t[g]);
+    w[1] = __ldg(&as_t[g]);
+  }
+  template <int SET>
+  __device__ __forceinline__ void pair(const IData &I, const float4 (&w)[JW],
+                                       float (&acc)[NA]) const {
+    const float dx = I.x - w[0].x, dy = I.y - w[0].y;
+    float nr2 = -dx * dx;
+    nr2 = fmaf(-dy, dy, nr2);
+    if (D == 3) {
+      const float dz = I.z - w[0].z;
+      nr2 = fmaf(-dz, dz, nr2);
+    }
+    const float K = DefKernel<ORDER>::val(nr2);
+    acc[0] = fmaf(K, w[1].x, acc[0]);
+    acc[1] = fmaf(K, w[1].y, acc[1]);
+    if (D == 3) acc[D - 1] = fmaf(K, w[1].z, acc[D - 1]);
+  }
+  __device__ double finalize(int p, int row, const double (&v)[NA]) const {
+    const PairDesc &P = pd[p];
+    if (row >= P.N) return 0.0;
+    const size_t g = (size_t)P.pt_off + row;
+    const double *a = x64 + P.var_off + ((size_t)t * P.N + row) * D;
+    double e = 0.0, qn[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      qn[d] = q64_t[g * D + d] + P.dt * v[d];
+      q64_n[g * D + d] = qn[d];
+      e += a[d] * v[d];
+      if (vlc64) vlc64[g * D + d] = v[d];
+    }
+    const double s = P.kscale;
+    qs_n[g] = make_float4((float)(qn[0] * s), (float)(qn[1] * s), (float)(qn[2] * s), 0.0f);
+    return e;
+  }
+  __device__ void write_tile(int p, int tile, double v) const {
+    tile_part[pd[p].itile_off + tile] = v;
+  }
+};
+
+// ------------------------------------------------------------------ backward
+// j data staged as 12 floats (3D) or 8 floats (2D):
+//   3D: (qx qy qz ux) (uy uz lx ly) (lz rx ry rz)     2D: (qx qy ux uy) (lx ly rx ry)
+// with u = a - p (kernel-product operand), l = a/2 - p, r = a (dq operands).
+
+template <int D, int ORDER>
+struct AdjointOp {
+  static constexpr int JW = (D == 3) ? 3 : 2;
+  static constexpr int NA = 2 * D;
+  static constexpr bool kTileSum = false;
+  static constexpr bool kTwoSets = false;
+  struct IData {
+    float q[D], l[D], r[D];
+  };
+  const PairDesc *pd;
+  const int *act;
+  const float4 *qs_t;  // scaled positions at t
+  const float4 *us_t;  // u_t = a_t - p
+  const float4 *ls_t;  // l_t = a_t / 2 - p
+  const float4 *as_t;  // r_t = a_t
+  double *p64;         // adjoint state (FP64), updated in place
+  const double *x64;   // FP64 alpha, variable layout
+  double *g64;         // gradient output, variable layout (nullptr: none)
+  float4 *us_n;        // u_{t-1} (written when t > 0)
+  float4 *ls_n;        // l_{t-1}
+  double *pdot64;      // optional raw dq output [NPtot * D] (standalone dq kernel)
+  int t;
+
+  __device__ bool active(int p) const { return act[p] != 0; }
+  __device__ int j_count(int p) const { return pd[p].Npad; }
+  __device__ int j_set(int, int) const { return 0; }
+  __device__ void load_i(int p, int row, IData &I) const {
+    const int g = pd[p].pt_off + row;
+    const float4 q = qs_t[g], l = ls_t[g], r = as_t[g];
+    I.q[0] = q.x; I.q[1] = q.y;
+    I.l[0] = l.x; I.l[1] = l.y;
+    I.r[0] = r.x; I.r[1] = r.y;
+    if (D == 3) {
+      I.q[D - 1] = q.z;
+      I.l[D - 1] = l.z;
+      I.r[D - 1] = r.z;
+    }
+  }
+  __device__ void load_j(int p, int j, float4 (&w)[JW]) const {
+    const int g = pd[p].pt_off + j;
+    const float4 q = __ldg(&qs_t[g]), u = __ldg(&us_t[g]), l = __ldg(&ls_t[g]),
+                 r = __ldg(&as_t[g]);
+    if (D == 3) {
+      w[0] = make_float4(q.x, q.y, q.z, u.x);
+      w[1] = make_float4(u.y, u.z, l.x, l.y);
+      w[JW - 1] = make_float4(l.z, r.x, r.y, r.z);
+    } else {
+      w[0] = make_float4(q.x, q.y, u.x, u.y);
+      w[1] = make_float4(l.x, l.y, r.x, r.y);
+    }
+  }
+  template <int SET>
+  __device__ __forceinline__ void pair(const IData &I, const float4 (&w)[JW],
+                                       float (&acc)[NA]) const {
+    float qj[D], uj[D], lj[D], rj[D];
+    if (D == 3) {
+      qj[0] = w[0].x; qj[1] = w[0].y; qj[D - 1] = w[0].z;
+      uj[0] = w[0].w; uj[1] = w[1].x; uj[D - 1] = w[1].y;
+      lj[0] = w[1].z; lj[1] = w[1].w; lj[D - 1] = w[JW - 1].x;
+      rj[0] = w[JW - 1].y; rj[1] = w[JW - 1].z; rj[D - 1] = w[JW - 1].w;
+    } else {
+      qj[0] = w[0].x; qj[1] = w[0].y;
+      uj[0] = w[0].z; uj[1] = w[0].w;
+      lj[0] = w[1].x; lj[1] = w[1].y;
+      rj[0] = w[1].z; rj[1] = w[1].w;
+    }
+    float dq[D];
+    float nr2 = 0.0f;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      dq[d] = I.q[d] - qj[d];
+      nr2 = fmaf(-dq[d], dq[d], nr2);
+    }
+    float K, Wt;
+    DefKernel<ORDER>::val_w(nr2, K, Wt);
+    float lr = I.l[0] * rj[0];
+#pragma unroll
+    for (int d = 1; d < D; ++d) lr = fmaf(I.l[d], rj[d], lr);
+#pragma unroll
+    for (int d = 0; d < D; ++d) lr = fmaf(lj[d], I.r[d], lr);
+    const float s = lr * Wt;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      acc[d] = fmaf(K, uj[d], acc[d]);
+      acc[D + d] = fmaf(s, dq[d], acc[D + d]);
+    }
+  }
+  __device__ double finalize(int p, int row, const double (&v)[NA]) const {
+    const PairDesc &P = pd[p];
+    if (row >= P.N) return 0.0;
+    const size_t g = (size_t)P.pt_off + row;
+    double pn[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const double pdot = P.pd_fac * v[D + d];
+      if (pdot64) pdot64[g * D + d] = pdot;
+      if (g64) g64[P.var_off + ((size_t)t * P.N + row) * D + d] = P.dt * v[d];
+      pn[d] = p64[g * D + d] - P.dt * pdot;
+      p64[g * D + d] = pn[d];
+    }
+    if (t > 0 && us_n) {
+      const double *a = x64 + P.var_off + ((size_t)(t - 1) * P.N + row) * D;
+      double u[3] = {0.0, 0.0, 0.0}, l[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        u[d] = a[d] - pn[d];
+        l[d] = 0.5 * a[d] - pn[d];
+      }
+      us_n[g] = make_float4((float)u[0], (float)u[1], (float)u[2], 0.0f);
+      ls_n[g] = make_float4((float)l[0], (float)l[1], (float)l[2], 0.0f);
+    }
+    return 0.0;
+  }
+  __device__ void write_tile(int, int, double) const {}
+};
+
+// ------------------------------------------------------------------ varifold
+// Deformed element i against every deformed (DD) and target (DT) element j:
+//   value   V_i   = a_i (S_DD + 2 S_DT),  S = sum k(c) b(ang) w_j
+//   centre  dc_i  = 2 a_i dc_fac sum kw(c) b w_j dc_scaled
+//   normal  dd_i  = f (sum k w_j b'(ang) n_j + n_i sum k w_j (b - ang b'))
+// with signed weights w_j = +a_j (deformed) / -a_j (target), f = 1 in 3D, 2 in 2D.
+// These are dqVf_Kernel's sums (Cpp/src/varifold3D.cpp:259-332,
+// Cpp/src/varifold2D.cpp:245-310) with grassmanFunction's derivative expanded: for
+// the unnormalised normal N (|N| = 2 a_i in 3D, a_i in 2D) its 1/|N| cancels the
+// a_i / (2 a_i) and the area derivative 0.5 n (3D) / n (2D).
+// j data: (c_scaled.xyz, w) (n.xyz, 0);  2D: (cx cy 0 w) (nx ny 0 0).
+// Accumulators: 0 S_DD, 1 S_DT, 2.. A (D), 2+D.. C (D), [2+2D B for non-Binet].
+
+template <int D, char CT, char DT>
+struct VarifoldOp {
+  static constexpr bool kBinet = (DT == 'B');
+  static constexpr int JW = 2;
+  static constexpr int NA = 2 + 2 * D + (kBinet ? 0 : 1);
+  static constexpr bool kTileSum = true;
+  static constexpr bool kTwoSets = true;
+  struct IData {
+    float c[D], n[D];
+  };
+  const PairDesc *pd;
+  const int *act;
+  const float4 *ec, *en;  // deformed: scaled centre + area, unit normal
+  const float4 *tc, *tn;  // target:   scaled centre - area, unit normal
+  const double *e64;      // deformed (n.xyz, area) FP64              [EDtot * 4]
+  double *dcdd;           // out: dc (D), dd (D) per deformed element [EDtot * 2D]
+  double *tile_part;      // varifold value per element tile
+  float ow2;              // 2 / dirKnlWidth^2 (Gaussian direction kernels)
+
+  __device__ bool active(int p) const { return act[p] != 0; }
+  __device__ int j_count(int p) const { return pd[p].Edpad + pd[p].Etpad; }
+  __device__ int j_set(int p, int j0) const { return j0 >= pd[p].Edpad ? 1 : 0; }
+  __device__ void load_i(int p, int row, IData &I) const {
+    const int g = pd[p].el_off + row;
+    const float4 c = ec[g], n = en[g];
+    I.c[0] = c.x; I.c[1] = c.y;
+    I.n[0] = n.x; I.n[1] = n.y;
+    if (D == 3) {
+      I.c[D - 1] = c.z;
+      I.n[D - 1] = n.z;
+    }
+  }
+  __device__ void load_j(int p, int j, float4 (&w)[JW]) const {
+    const PairDesc &P = pd[p];
+    if (j < P.Edpad) {
+      w[0] = __ldg(&ec[P.el_off + j]);
+      w[1] = __ldg(&en[P.el_off + j]);
+    } else {
+      w[0] = __ldg(&tc[P.tg_off + j - P.Edpad]);
+      w[1] = __ldg(&tn[P.tg_off + j - P.Edpad]);
+    }
+  }
+  template <int SET>
+  __device__ __forceinline__ void pair(const IData &I, const float4 (&w)[JW],
+                                       float (&acc)[NA]) const {
+    const float cj[3] = {w[0].x, w[0].y, w[0].z};
+    const float nj[3] = {w[1].x, w[1].y, w[1].z};
+    float dc[D];
+    float nr2 = 0.0f, ang = 0.0f;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      dc[d] = I.c[d] - cj[d];
+      nr2 = fmaf(-dc[d], dc[d], nr2);
+      ang = fmaf(I.n[d], nj[d], ang);
+    }
+    float k, kg;
+    CenKernel<CT>::val_w(nr2, k, kg);
+    const float kw = k * w[0].w;
+    if (kBinet) {
+      const float t1 = kw * ang;  // k w b'/2
+      const float tb = t1 * ang;  // k w b
+      acc[SET] += tb;
+      const float cg_ = (CT == 'G') ? tb : tb * k;  // kg w b
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        acc[2 + d] = fmaf(t1, nj[d], acc[2 + d]);
+        acc[2 + D + d] = fmaf(cg_, dc[d], acc[2 + D + d]);
+      }
+    } else {
+      float b, db;
+      DirKernel<DT>::val_d(ang, ow2, b, db);
+      const float tb = kw * b;
+      const float td = kw * db;
+      acc[SET] += tb;
+      const float cg_ = (CT == 'G') ? tb : tb * k;
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        acc[2 + d] = fmaf(td, nj[d], acc[2 + d]);
+        acc[2 + D + d] = fmaf(cg_, dc[d], acc[2 + D + d]);
+      }
+      acc[NA - 1] = fmaf(-ang, td, acc[NA - 1] + tb);
+    }
+  }
+  __device__ double finalize(int p, int row, const double (&v)[NA]) const {
+    const PairDesc &P = pd[p];
+    if (row >= P.Ed) return 0.0;
+    const size_t g = (size_t)P.el_off + row;
+    const double *e = e64 + g * 4;
+    const double ai = e[3];
+    const double fac = (D == 3) ? 1.0 : 2.0;
+    double A[3], B;
+    if (kBinet) {
+      // b' = 2 ang, b - ang b' = -ang^2: A = 2 sum t1 n_j, B = -(S_DD + S_DT)
+      for (int d = 0; d < D; ++d) A[d] = 2.0 * v[2 + d];
+      B = -(v[0] + v[1]);
+    } else {
+      for (int d = 0; d < D; ++d) A[d] = v[2 + d];
+      B = v[NA - 1];
+    }
+    double *o = dcdd + g * (2 * D);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      o[d] = 2.0 * ai * P.dc_fac * v[2 + D + d];
+      o[D + d] = fac * (A[d] + B * e[d]);
+    }
+    return ai * (v[0] + 2.0 * v[1]);
+  }
+  __device__ void write_tile(int p, int tile, double v) const {
+    tile_part[pd[p].etile_off + tile] = v;
+  }
+};
+
+// --------------------------------------------------------- per-element kernels
+
+// landmarksToVarifoldKernel (Cpp/src/varifold3D.cpp:8-39, varifold2D.cpp:8-32), in
+// FP64 from the final positions; writes the FP32 sweep operands and FP64 copies.
+template <int D>
+__global__ void geometry_kernel(const PairDesc *__restrict__ pd, const int *__restrict__ act,
+                                const int4 *__restrict__ elm, int n_elm,
+                                const double *__restrict__ q64, float4 *ec, float4 *en,
+                                double *e64) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_elm) return;
+  const int4 ev = elm[g];
+  if (ev.w < 0 || !act[ev.w]) return;
+  const PairDesc &P = pd[ev.w];
+  double c[3] = {0, 0, 0}, n[3] = {0, 0, 0}, a;
+  if (D == 3) {
+    const double *q0 = q64 + (size_t)ev.x * 3, *q1 = q64 + (size_t)ev.y * 3,
+                 *q2 = q64 + (size_t)ev.z * 3;
+    double u[3], w[3];
+    for (int d = 0; d < 3; ++d) {
+      c[d] = (q0[d] + q1[d] + q2[d]) / 3.0;
+      u[d] = q1[d] - q0[d];
+      w[d] = q2[d] - q0[d];
+    }
+    n[0] = u[1] * w[2] - u[2] * w[1];
+    n[1] = -u[0] * w[2] + u[2] * w[0];
+    n[2] = u[0] * w[1] - u[1] * w[0];
+    const double len = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+    for (int d = 0; d < 3; ++d) n[d] /= len;
+    a = 0.5 * len;
+  } else {
+    const double *q0 = q64 + (size_t)ev.x * 2, *q1 = q64 + (size_t)ev.y * 2;
+    for (int d = 0; d < 2; ++d) {
+      c[d] = 0.5 * (q0[d] + q1[d]);
+      n[d] = q1[d] - q0[d];
+    }
+    const double len = sqrt(n[0] * n[0] + n[1] * n[1]);
+    n[0] /= len;
+    n[1] /= len;
+    a = len;
+  }
+  const double s = P.cscale;
+  ec[g] = make_float4((float)(c[0] * s), (float)(c[1] * s), (float)(c[2] * s), (float)a);
+  en[g] = make_float4((float)n[0], (float)n[1], (float)n[2], 0.0f);
+  double *e = e64 + (size_t)g * 4;
+  e[0] = n[0];
+  e[1] = n[1];
+  e[2] = n[2];
+  e[3] = a;
+}
+
+// dqVfdGatherKernel (Cpp/src/varifold3D.cpp:359-391, varifold2D.cpp:337-359) fused
+// with the start of the adjoint (Cpp/src/objgrd.cpp:67): p = -w dV/dq, and the
+// operands u, l of the first backward step.  One thread per (padded) vertex.
+template <int D>
+__global__ void gather_kernel(const PairDesc *__restrict__ pd, const int *__restrict__ act,
+                              const int *__restrict__ pt_pair, int n_pt,
+                              const int *__restrict__ adj_ptr, const int4 *__restrict__ adj,
+                              const double *__restrict__ dcdd, const double *__restrict__ q64T,
+                              const double *__restrict__ x64, double *p64, float4 *us_n,
+                              float4 *ls_n, double *dq_out, int T) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_pt) return;
+  const int p = pt_pair[g];
+  if (p < 0 || !act[p]) return;
+  const PairDesc &P = pd[p];
+  const int row = g - P.pt_off;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int k = adj_ptr[g]; k < adj_ptr[g + 1]; ++k) {
+    const int4 e = adj[k];
+    const double *o = dcdd + (size_t)e.x * (2 * D);
+    if (D == 3) {
+      const double *qa = q64T + (size_t)e.y * 3, *qb = q64T + (size_t)e.z * 3;
+      const double ab[3] = {qa[0] - qb[0], qa[1] - qb[1], qa[2] - qb[2]};
+      const double *dd = o + 3;
+      const double x0 = dd[1] * ab[2] - dd[2] * ab[1];
+      const double x1 = -dd[0] * ab[2] + dd[2] * ab[0];
+      const double x2 = dd[0] * ab[1] - dd[1] * ab[0];
+      acc[0] += o[0] / 3.0 + x0;
+      acc[1] += o[1] / 3.0 + x1;
+      acc[2] += o[2] / 3.0 + x2;
+    } else {
+      acc[0] += 0.5 * o[0] + e.y * o[2];
+      acc[1] += 0.5 * o[1] + e.y * o[3];
+    }
+  }
+  double pn[3] = {0.0, 0.0, 0.0};
+  for (int d = 0; d < D; ++d) {
+    if (dq_out) dq_out[(size_t)g * D + d] = acc[d];
+    pn[d] = -P.dis_wgt * acc[d];
+    p64[(size_t)g * D + d] = pn[d];
+  }
+  if (us_n && T > 0) {
+    const double *a = x64 + P.var_off + ((size_t)(T - 1) * P.N + row) * D;
+    double u[3] = {0, 0, 0}, l[3] = {0, 0, 0};
+    for (int d = 0; d < D; ++d) {
+      u[d] = a[d] - pn[d];
+      l[d] = 0.5 * a[d] - pn[d];
+    }
+    us_n[g] = make_float4((float)u[0], (float)u[1], (float)u[2], 0.0f);
+    ls_n[g] = make_float4((float)l[0], (float)l[1], (float)l[2], 0.0f);
+  }
+}
+
+// E = dt/2 sum_t a_t.v_t + w (V_DD,DT + V_TT)   (Cpp/src/objgrd.cpp:65).  One CTA
+// per pair, partials summed in fixed order.
+__global__ void objective_kernel(const PairDesc *__restrict__ pd, const int *__restrict__ act,
+                                 const double *__restrict__ reg_part, int ntile_tot,
+                                 const double *__restrict__ vfd_part, int T, PairState *st,
+                                 double *f_out) {
+  __shared__ double scr[32];
+  const int p = blockIdx.x;
+  if (!act[p]) return;
+  const PairDesc &P = pd[p];
+  const int nt = P.Npad / kTile, ne = P.Edpad / kTile;
+  double r = 0.0, v = 0.0;
+  for (int k = threadIdx.x; k < T * nt; k += blockDim.x) {
+    const int t = k / nt, i = k - t * nt;
+    r += reg_part[(size_t)t * ntile_tot + P.itile_off + i];
+  }
+  for (int k = threadIdx.x; k < ne; k += blockDim.x) v += vfd_part[P.etile_off + k];
+  const double R = block_sum(r, scr);
+  const double V = block_sum(v, scr);
+  if (threadIdx.x == 0) {
+    const double f = P.dt * 0.5 * R + P.dis_wgt * (V + P.tt);
+    if (st) st[p].f_try = f;
+    if (f_out) f_out[p] = f;
+  }
+}
+
+// Target self-term in FP64, once per context (the constant third double loop of
+// dqVf_Kernel, Cpp/src/varifold3D.cpp:334-354).  Block partials per (pair, i-block).
+template <int D, char CT, char DT>
+__global__ void target_self_kernel(const double *__restrict__ tgt, int Et, double cw, double dw,
+                                   double *part) {
+  __shared__ double scr[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double s = 0.0;
+  if (i < Et) {
+    const double *ti = tgt + (size_t)i * 8;
+    const double w2 = cw * cw, ow2 = 2.0 / (dw * dw);
+    for (int j = 0; j < Et; ++j) {
+      const double *tj = tgt + (size_t)j * 8;
+      double r2 = 0.0, ang = 0.0;
+      for (int d = 0; d < D; ++d) {
+        const double x = ti[d] - tj[d];
+        r2 += x * x;
+        ang += ti[3 + d] * tj[3 + d];
+      }
+      const double k = (CT == 'G') ? exp(-r2 / w2) : 1.0 / (1.0 + r2 / w2);
+      double b;
+      if (DT == 'B') b = ang * ang;
+      else if (DT == 'L') b = ang;
+      else if (DT == 'O') b = exp((ang - 1.0) * ow2);
+      else b = exp((ang * ang - 1.0) * ow2);
+      s += k * b * ti[6] * tj[6];
+    }
+  }
+  const double tot = block_sum(s, scr);
+  if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
+
+}  // namespace lddmm

@@ -1,0 +1,149 @@
+// All-pairs sweep skeleton shared by the shooting, adjoint and varifold kernels.
+//
+// Work decomposition (one launch per sweep, every pair of the batch in it):
+//   item    = (pair, i-tile of kTile = 64 rows); the item list is built on the host,
+//             largest pairs first.
+//   cluster = S CTAs on one item (thread-block cluster along x); CTA rank r takes
+//             every S-th group of W j-sub-tiles.
+//   CTA     = W warps; every warp owns all 64 rows of the tile (2 rows per lane) and
+//             its own 32-point j-sub-tiles, staged warp-privately in shared memory
+//             with the next sub-tile prefetched into registers, so warps never wait
+//             on each other inside the j loop.
+// Each 32-pair sub-tile is summed in plain FP32 and folded into a (hi, lo) TwoSum
+// accumulator.  Warps are combined in FP64 through shared memory, the cluster's
+// CTAs through distributed shared memory (DSMEM) in fixed rank order, so every
+// result is bit-reproducible run to run.  Rank 0 of the cluster finalises the rows
+// and reduces one FP64 value per tile (energy / varifold value) in fixed order.
+//
+// An Op supplies:
+//   JW, NA            float4 words per staged j point; accumulators per row
+//   IData             per-row registers
+//   active(p)         evaluate pair p in this sweep
+//   load_i(p, row, I) load row data
+//   j_count(p)        padded j extent (multiple of kTile)
+//   j_set(p, j0)      0/1 class of the sub-tile starting at j0 (warp-uniform)
+//   load_j(p, j, w)   global -> registers, one j point per lane
+//   kTwoSets          j_set can return 1
+//   pair<SET>(I, w, acc)        accumulate one pair interaction
+//   finalize(p, row, acc)       consume the full FP64 row sums; returns a value
+//                               that is summed over the tile
+//   write_tile(p, tile, v)      store the tile sum
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+
+namespace lddmm {
+
+namespace cg = cooperative_groups;
+
+// One staged 32-point sub-tile against the warp's two rows.  SET is the
+// compile-time class of the sub-tile (the varifold's deformed / target halves), so
+// the accumulator index is static and the arrays stay in registers.
+template <int SET, class Op>
+__device__ __forceinline__ void run_sub(const Op &op, const float4 (*sj)[kSub],
+                                        const typename Op::IData &I0,
+                                        const typename Op::IData &I1, float (&a0)[Op::NA],
+                                        float (&a1)[Op::NA]) {
+#pragma unroll 8
+  for (int jj = 0; jj < kSub; ++jj) {
+    float4 w[Op::JW];
+#pragma unroll
+    for (int x = 0; x < Op::JW; ++x) w[x] = sj[x][jj];
+    op.template pair<SET>(I0, w, a0);
+    op.template pair<SET>(I1, w, a1);
+  }
+}
+
+template <class Op, int W>
+__global__ void __launch_bounds__(W * 32) sweep_kernel(const Op op, const int2 *__restrict__ items,
+                                                       int S) {
+  constexpr int JW = Op::JW;
+  constexpr int NA = Op::NA;
+  __shared__ float4 s_j[W][JW][kSub];
+  __shared__ double s_red[W][kTile][NA];
+  __shared__ double s_cta[kTile][NA];
+  __shared__ double s_scr[W];
+
+  const int item = blockIdx.x / S;
+  const int rank = blockIdx.x - item * S;
+  const int2 it = items[item];
+  const int p = it.x, tile = it.y;
+  if (!op.active(p)) return;  // identical for every CTA of the cluster
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  typename Op::IData I0, I1;
+  op.load_i(p, tile * kTile + lane, I0);
+  op.load_i(p, tile * kTile + 32 + lane, I1);
+
+  float hi0[NA], lo0[NA], hi1[NA], lo1[NA];
+#pragma unroll
+  for (int a = 0; a < NA; ++a) hi0[a] = lo0[a] = hi1[a] = lo1[a] = 0.0f;
+
+  const int nsub = op.j_count(p) / kSub;
+  const int step = S * W;
+  int k = rank * W + warp;
+  float4 nxt[JW];
+  if (k < nsub) op.load_j(p, k * kSub + lane, nxt);
+  while (k < nsub) {
+    __syncwarp();
+#pragma unroll
+    for (int x = 0; x < JW; ++x) s_j[warp][x][lane] = nxt[x];
+    __syncwarp();
+    const int kn = k + step;
+    const int set = op.j_set(p, k * kSub);
+    if (kn < nsub) op.load_j(p, kn * kSub + lane, nxt);
+    float a0[NA], a1[NA];
+#pragma unroll
+    for (int a = 0; a < NA; ++a) a0[a] = a1[a] = 0.0f;
+    if (Op::kTwoSets && set)
+      run_sub<1>(op, s_j[warp], I0, I1, a0, a1);
+    else
+      run_sub<0>(op, s_j[warp], I0, I1, a0, a1);
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+      two_sum_acc(hi0[a], lo0[a], a0[a]);
+      two_sum_acc(hi1[a], lo1[a], a1[a]);
+    }
+    k = kn;
+  }
+
+#pragma unroll
+  for (int a = 0; a < NA; ++a) {
+    s_red[warp][lane][a] = (double)hi0[a] + (double)lo0[a];
+    s_red[warp][32 + lane][a] = (double)hi1[a] + (double)lo1[a];
+  }
+  __syncthreads();
+  double v[NA];
+  if (threadIdx.x < kTile) {
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+      double s = 0.0;
+      for (int w = 0; w < W; ++w) s += s_red[w][threadIdx.x][a];
+      v[a] = s;
+      s_cta[threadIdx.x][a] = s;
+    }
+  }
+  if (S > 1) {
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    if (rank == 0 && threadIdx.x < kTile) {
+      for (int r = 1; r < S; ++r) {
+        const double *rem = cluster.map_shared_rank(&s_cta[0][0], r);
+#pragma unroll
+        for (int a = 0; a < NA; ++a) v[a] += rem[threadIdx.x * NA + a];
+      }
+    }
+    cluster.sync();
+  }
+  if (rank != 0) return;
+  double e = 0.0;
+  if (threadIdx.x < kTile) e = op.finalize(p, tile * kTile + threadIdx.x, v);
+  if (Op::kTileSum) {
+    const double tot = block_sum(e, s_scr);
+    if (threadIdx.x == 0) op.write_tile(p, tile, tot);
+  }
+}
+
+}  // namespace lddmm

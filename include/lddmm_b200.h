@@ -187,6 +187,27 @@ int lddmm_dq_kernel(int dim, int n, const double *q, const double *l, const doub
                     int knl_order, double knl_width, double *dq);
 int lddmm_varifold(const lddmm_problem *prob, const double *nde, double *val, double *dq);
 
+/* Allocation-free v_i = sum_j K(q_i, q_j) a_j.  No counterpart in the reference.
+ *
+ * For callers that must not have the library call cudaMalloc/cudaFree: a MEX
+ * function working on MATLAB gpuArray data (the device memory belongs to MATLAB's
+ * allocator, which the library cannot see), a framework whose caching allocator owns
+ * the GPU, or a host loop that cannot afford the device-wide synchronisation that
+ * cudaFree implies.  d_q, d_a (inputs, dim x n) and d_v (output, dim x n) are device
+ * buffers the caller owns; the working set lives in one fixed array of about 2.3 MB
+ * compiled into the library, which every GPU that loads the library holds until the
+ * process exits.  Nothing is allocated.
+ *
+ * Limit: 1 <= n <= LDDMM_NOALLOC_MAX_POINTS; larger n returns LDDMM_ERR_ARG.
+ * The first call on a device looks up the array's device address (with that device
+ * current); make that first call before any stream capture.  Every call shares the
+ * array: calls that overlap on the GPU (other streams, other host threads) race and
+ * give wrong results; each call clears what must start at zero.  Asynchronous on
+ * `stream` (a cudaStream_t, NULL for the default stream). */
+#define LDDMM_NOALLOC_MAX_POINTS 32768
+int lddmm_multiply_kernel_noalloc(int dim, int n, const double *d_q, const double *d_a,
+                                  int knl_order, double knl_width, double *d_v, void *stream);
+
 /* Measurement.  Evaluates the objective `reps` times at the context's current
  * trial point with CUDA events on the context stream around every sweep launch and
  * writes average milliseconds per launch: ms4[0] shooting step, ms4[1] fused adjoint

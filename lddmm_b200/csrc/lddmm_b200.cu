@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <memory>
+#include <mutex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -1336,6 +1337,155 @@ extern "C" int lddmm_LDDMM(int dim, int nde_num, int dfm_elm_num, int dfm_elm_if
   o.vbs_flg = Verbose;
   lddmm_result r;
   return lddmm_lbfgs(ctx, &o, optAlpVec, &r);
+}
+
+// ====================================================== allocation-free entry
+//
+// lddmm_multiply_kernel_noalloc: the shooting sweep for one point set with its working
+// set in a file-scope device array instead of cudaMalloc'd memory.  Byte layout of the
+// array (offsets 256-aligned): PairDesc | active flag | i-tile items | tile partials |
+// scaled positions | FP32 momenta | next positions (scaled FP32, FP64).
+
+constexpr int kNaMax = LDDMM_NOALLOC_MAX_POINTS;
+constexpr int kNaTiles = kNaMax / kTile;
+constexpr size_t kNaPd = 0;
+constexpr size_t kNaAct = 256;
+constexpr size_t kNaItems = 512;
+constexpr size_t kNaTile = kNaItems + sizeof(int2) * kNaTiles;
+constexpr size_t kNaQs = kNaTile + sizeof(double) * kNaTiles;
+constexpr size_t kNaAs = kNaQs + sizeof(float4) * kNaMax;
+constexpr size_t kNaQsn = kNaAs + sizeof(float4) * kNaMax;
+constexpr size_t kNaQ64n = kNaQsn + sizeof(float4) * kNaMax;
+constexpr size_t kNaBytes = kNaQ64n + sizeof(double) * 3 * kNaMax;
+static_assert(sizeof(PairDesc) <= 256, "PairDesc must fit its slot");
+static_assert(kNaTile % 256 == 0 && kNaQs % 256 == 0 && kNaAs % 256 == 0 &&
+                  kNaQsn % 256 == 0 && kNaQ64n % 256 == 0,
+              "scratch slots must stay 256-byte aligned");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+// Host-side device addresses of g_noalloc_scratch, one per device ordinal (the symbol
+// name itself is only a host stand-in and must never be passed to a kernel).
+static std::mutex g_noalloc_mu;
+static unsigned char *g_noalloc_addr[128];
+
+static int noalloc_scratch(int dev, unsigned char **out) {
+  if (dev < 0 || dev >= 128) {
+    set_err("lddmm_multiply_kernel_noalloc: device ordinal %d out of range", dev);
+    return LDDMM_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      set_err("lddmm_multiply_kernel_noalloc: cudaGetSymbolAddress failed: %s",
+              cudaGetErrorString(e));
+      return LDDMM_ERR_CUDA;
+    }
+    g_noalloc_addr[dev] = static_cast<unsigned char *>(p);
+  }
+  *out = g_noalloc_addr[dev];
+  return 0;
+}
+
+// Fills the scratch for one call: pair descriptor, active flag, tile items, and the
+// FP32 operands with the padding rows cleared (the array keeps the previous call's
+// contents).
+__global__ void noalloc_prepare_kernel(unsigned char *scratch, PairDesc desc,
+                                       const double *__restrict__ q,
+                                       const double *__restrict__ a, int n, int npad, int D) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float4 *qs = reinterpret_cast<float4 *>(scratch + kNaQs);
+  float4 *as = reinterpret_cast<float4 *>(scratch + kNaAs);
+  if (i == 0) {
+    *reinterpret_cast<PairDesc *>(scratch + kNaPd) = desc;
+    *reinterpret_cast<int *>(scratch + kNaAct) = 1;
+  }
+  if (i < npad / kTile) reinterpret_cast<int2 *>(scratch + kNaItems)[i] = make_int2(0, i);
+  if (i >= npad) return;
+  float x[3] = {0, 0, 0}, y[3] = {0, 0, 0};
+  if (i < n)
+    for (int d = 0; d < D; ++d) {
+      x[d] = (float)(q[(size_t)i * D + d] * desc.kscale);
+      y[d] = (float)a[(size_t)i * D + d];
+    }
+  qs[i] = make_float4(x[0], x[1], x[2], 0.0f);
+  as[i] = make_float4(y[0], y[1], y[2], 0.0f);
+}
+
+template <int D, int ORDER>
+static cudaError_t noalloc_sweep(unsigned char *scratch, const double *q, const double *a,
+                                 double *v, int ntiles, cudaStream_t stream) {
+  ShootOp<D, ORDER> op;
+  op.pd = reinterpret_cast<const PairDesc *>(scratch + kNaPd);
+  op.act = reinterpret_cast<const int *>(scratch + kNaAct);
+  op.qs_t = reinterpret_cast<const float4 *>(scratch + kNaQs);
+  op.as_t = reinterpret_cast<const float4 *>(scratch + kNaAs);
+  op.q64_t = q;
+  op.q64_n = reinterpret_cast<double *>(scratch + kNaQ64n);
+  op.qs_n = reinterpret_cast<float4 *>(scratch + kNaQsn);
+  op.x64 = a;
+  op.vlc64 = v;
+  op.tile_part = reinterpret_cast<double *>(scratch + kNaTile);
+  op.t = 0;
+  return launch_sweep(op, reinterpret_cast<const int2 *>(scratch + kNaItems), ntiles,
+                      default_cluster(ntiles), stream);
+}
+
+extern "C" int lddmm_multiply_kernel_noalloc(int dim, int n, const double *d_q,
+                                             const double *d_a, int knl_order,
+                                             double knl_width, double *d_v, void *stream) {
+  if (dim != 2 && dim != 3) {
+    set_err("lddmm_multiply_kernel_noalloc: dim must be 2 or 3");
+    return LDDMM_ERR_ARG;
+  }
+  if (n < 1 || n > kNaMax) {
+    set_err("lddmm_multiply_kernel_noalloc: n = %d outside 1..%d (LDDMM_NOALLOC_MAX_POINTS)",
+            n, kNaMax);
+    return LDDMM_ERR_ARG;
+  }
+  if (!d_q || !d_a || !d_v || !(knl_width > 0)) {
+    set_err("lddmm_multiply_kernel_noalloc: null buffer or non-positive width");
+    return LDDMM_ERR_ARG;
+  }
+  if (knl_order < -1 || knl_order > 4 || (dim == 2 && knl_order != -1)) {
+    set_err("lddmm_multiply_kernel_noalloc: kernel order %d in %dD not supported", knl_order,
+            dim);
+    return LDDMM_ERR_UNSUPPORTED;
+  }
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  unsigned char *scratch = nullptr;
+  const int rc = noalloc_scratch(dev, &scratch);
+  if (rc) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  PairDesc desc;
+  std::memset(&desc, 0, sizeof(desc));
+  desc.N = n;
+  desc.Npad = pad_to(n, kTile);
+  desc.var_num = (long long)dim * n;
+  desc.dt = 1.0;
+  def_kernel_scales(knl_order, knl_width, &desc.kscale, &desc.pd_fac);
+  const int ntiles = desc.Npad / kTile;
+  noalloc_prepare_kernel<<<(desc.Npad + 255) / 256, 256, 0, st>>>(scratch, desc, d_q, d_a, n,
+                                                                   desc.Npad, dim);
+  CU(cudaGetLastError());
+  cudaError_t e = cudaErrorInvalidValue;
+  if (dim == 2) {
+    e = noalloc_sweep<2, -1>(scratch, d_q, d_a, d_v, ntiles, st);
+  } else {
+    switch (knl_order) {
+      case -1: e = noalloc_sweep<3, -1>(scratch, d_q, d_a, d_v, ntiles, st); break;
+      case 0: e = noalloc_sweep<3, 0>(scratch, d_q, d_a, d_v, ntiles, st); break;
+      case 1: e = noalloc_sweep<3, 1>(scratch, d_q, d_a, d_v, ntiles, st); break;
+      case 2: e = noalloc_sweep<3, 2>(scratch, d_q, d_a, d_v, ntiles, st); break;
+      case 3: e = noalloc_sweep<3, 3>(scratch, d_q, d_a, d_v, ntiles, st); break;
+      case 4: e = noalloc_sweep<3, 4>(scratch, d_q, d_a, d_v, ntiles, st); break;
+    }
+  }
+  CU(e);
+  return 0;
 }
 
 // ============================================================ FP32 probe

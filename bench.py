@@ -38,11 +38,14 @@ WORKLOAD = "sphere2cube: icosphere 2562 v / 5120 t -> cube 12288 t, Matern nu=3/
            "varifold G(0.15) x Binet, T=20, L-BFGS m=5, <=500 iterations"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 
-# Objective evaluations of one registration of this workload, used to turn the
-# reference's per-evaluation CPU time into registrations/s (the reference cannot run
-# a whole registration inside the bench's time budget).  Measured by this bench on
-# B200 (FP32 path, 500 iterations); the FP64 path takes a similar count.
-EVALS_PER_REGISTRATION = 520
+# The FP64 registration of this workload (CPU oracle, 500 iterations; generator
+# tests/golden/make_c2_reference.py): its objective is what a registration has to
+# reach (within 1e-5 relative), and its evaluation count turns the reference's
+# per-evaluation CPU time into registrations/s (a whole reference registration does
+# not fit the bench's time budget).
+with open(os.path.join(ROOT, "tests", "golden", "sphere2cube_fp64_500.json")) as _f:
+    FP64_REGISTRATION = json.load(_f)
+EVALS_PER_REGISTRATION = int(FP64_REGISTRATION["evals"])
 
 
 def parse():
@@ -53,6 +56,15 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--itr", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", choices=["registration", "objgrd"], default="registration",
+                    help="objgrd: only time device-resident objective+gradient evaluations "
+                         "(the command the ncu captures in profiles/ use)")
+    ap.add_argument("--evals", type=int, default=20)
+    ap.add_argument("--subdiv", type=int, default=4,
+                    help="objgrd mode: icosphere subdivisions of the source (4: 2562 points)")
+    ap.add_argument("--persistent", type=int, default=0,
+                    help="objgrd mode: 1 persistent time-loop sweeps, -1 per-step launches, "
+                         "0 automatic")
     return ap.parse_args()
 
 
@@ -215,7 +227,10 @@ def run_ours(args):
     from lddmm_b200 import _lib, api
 
     P = workload()
-    stream = torch.cuda.current_stream()
+    # one explicit stream shared by torch and the context, so that the CUDA events
+    # below bracket the context's kernels
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx = api.Context(P, stream=stream.cuda_stream, device=local)
     nvar = ctx.var_total
     d_alp = torch.zeros(nvar, dtype=torch.float64, device="cuda")
@@ -361,6 +376,9 @@ def run_ours(args):
                        "l2": "256 MiB memset before every registration",
                        "iters": iters, "status": status, "evals_per_registration": evals_per_reg,
                        "f_final": f_final, "rel_err_f_vs_fp64_oracle": rel_f,
+                       "f_fp64_registration": FP64_REGISTRATION["f"],
+                       "rel_diff_vs_fp64_registration":
+                           abs(f_final - FP64_REGISTRATION["f"]) / abs(FP64_REGISTRATION["f"]),
                        "gpair_interactions_per_s": gpairs,
                        "cluster": list(ctx.launch_config()),
                        "sweep_ms": {k: round(v, 5) for k, v in sweeps.items()}},
@@ -383,8 +401,50 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_objgrd(args):
+    """Device-resident objective + gradient evaluations of the workload at a fixed
+    momentum field; prints ms per evaluation."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from lddmm_b200 import _lib, api, problem
+
+    P = problem.sphere_to_cube(subdiv=args.subdiv)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx = api.Context(P, stream=stream.cuda_stream, persistent=args.persistent)
+    alp = torch.from_numpy(np.random.default_rng(0).normal(size=P.var_num) * 0.01).cuda()
+    f = torch.zeros(1, dtype=torch.float64, device="cuda")
+    g = torch.zeros_like(alp)
+
+    def ev():
+        _lib.check(_lib.lib.lddmm_objgrd_device(ctx.handle, C.c_void_p(alp.data_ptr()),
+                                                C.c_void_p(f.data_ptr()),
+                                                C.c_void_p(g.data_ptr()), 1))
+
+    for _ in range(max(args.warmup, 1)):
+        ev()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.evals):
+        ev()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.evals
+    print(json.dumps({"mode": "objgrd", "points": P.nde_num, "ms_per_eval": ms,
+                      "f": float(f.item()), "cluster": list(ctx.launch_config())}), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.mode == "objgrd":
+        run_objgrd(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -103,6 +103,9 @@ typedef struct lddmm_config {
 	int use_graph;            /* 1 (default): capture the L-BFGS cycle in a CUDA graph */
 	void *stream;             /* cudaStream_t to run on; NULL: the context creates one */
 	int device;               /* CUDA device ordinal (default 0) */
+	int persistent;           /* time loops as one persistent cooperative launch per
+	                             direction: 1 on, -1 off, 0 automatic (on when one step
+	                             of the batch does not fill the GPU) */
 } lddmm_config;
 
 /* Per-pair outcome of lddmm_lbfgs. */

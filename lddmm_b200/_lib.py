@@ -57,7 +57,7 @@ class Opt(C.Structure):
 class Config(C.Structure):
     _fields_ = [("cluster_shoot", C.c_int), ("cluster_adjoint", C.c_int),
                 ("cluster_varifold", C.c_int), ("autotune", C.c_int), ("use_graph", C.c_int),
-                ("stream", C.c_void_p), ("device", C.c_int)]
+                ("stream", C.c_void_p), ("device", C.c_int), ("persistent", C.c_int)]
 
 
 class Result(C.Structure):

@@ -39,7 +39,7 @@ class Context:
     """A batch of pairs on the GPU (``lddmm_ctx``)."""
 
     def __init__(self, problems, cluster=(0, 0, 0), autotune=False, use_graph=True,
-                 stream=None, device=0):
+                 stream=None, device=0, persistent=0):
         if isinstance(problems, Problem):
             problems = [problems]
         self.problems = list(problems)
@@ -47,7 +47,7 @@ class Context:
         arr = (_lib.Problem * len(self.problems))(
             *[_problem_struct(P, keep) for P in self.problems])
         cfg = _lib.Config(cluster[0], cluster[1], cluster[2], 1 if autotune else 0,
-                          1 if use_graph else -1, stream, device)
+                          1 if use_graph else -1, stream, device, persistent)
         h = C.c_void_p()
         check(lib.lddmm_ctx_create(arr, len(self.problems), C.byref(cfg), C.byref(h)))
         self._h = h

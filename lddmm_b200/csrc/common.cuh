@@ -37,6 +37,19 @@ __device__ __forceinline__ float rcpf_approx(float x) {
   return y;
 }
 
+// ------------------------------------------- programmatic dependent launch
+// Kernels of the objective sweep and the L-BFGS cycle are launched with
+// programmatic stream serialisation: a kernel may start while its predecessor is
+// still running.  Every such kernel executes pdl_wait() before it reads anything a
+// predecessor writes and before any early return (so a grid never completes ahead
+// of its predecessor), and pdl_trigger() to let its own successor start launching.
+// Without the launch attribute both are no-ops.
+
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // ------------------------------------------------- compensated accumulation
 // Knuth's TwoSum: hi + lo carries the running sum exactly up to the rounding of
 // the final hi + lo.  Tile partials (32 terms, plain FP32) are folded in here, so

@@ -27,7 +27,8 @@ struct PairDesc {
   int pt_off;         // first point in point arrays
   int el_off;         // first deformed element in element arrays
   int tg_off;         // first target element in target arrays
-  int itile_off;      // first i-tile of this pair (shoot/adjoint partials)
+  int itile_off;      // first 64-row i-tile of this pair (per-step sweep partials)
+  int grp_off;        // first 8-row group of this pair (persistent sweep partials)
   int etile_off;      // first element tile of this pair (varifold partials)
   int adj_off;        // first entry of this pair's vertex CSR pointer array
   int chunk_off, nchunk;  // vector-pass chunks of this pair

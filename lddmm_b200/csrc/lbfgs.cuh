@@ -69,6 +69,8 @@ __device__ __forceinline__ void store_trial_f32(const VecArgs &A, const PairDesc
 __global__ void __launch_bounds__(kVecThreads) vec_pass_kernel(VecArgs A, int mode, int k) {
   __shared__ double s_scal[4];
   __shared__ double s_scr[kVecThreads / 32];
+  pdl_wait();
+  pdl_trigger();
   const int c = blockIdx.x;
   const int p = A.chunk_pair[c];
   const PairDesc &P = A.pd[p];
@@ -248,6 +250,8 @@ __device__ __forceinline__ double serial_partial(const double *part, int c0, int
 // After POST.  One thread per pair.  Records (f, |g|, step, evals) per iteration.
 __global__ void decide_kernel(const PairDesc *__restrict__ pd, PairState *st, int P,
                               const double *__restrict__ part, OptParams o, double *rec) {
+  pdl_wait();
+  pdl_trigger();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   PairState &S = st[p];
@@ -341,6 +345,8 @@ __global__ void decide_kernel(const PairDesc *__restrict__ pd, PairState *st, in
 // (lineSearch.cpp:34-55) and sets the evaluation flags for the next sweep.
 __global__ void ls_init_kernel(const PairDesc *__restrict__ pd, PairState *st, int P,
                                const double *__restrict__ part, int *act) {
+  pdl_wait();
+  pdl_trigger();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P) return;
   PairState &S = st[p];

@@ -4,6 +4,7 @@
 #include <cmath>
 #include <memory>
 #include <mutex>
+#include <utility>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -16,6 +17,7 @@
 #include "layout.h"
 #include "lbfgs.cuh"
 #include "ops.cuh"
+#include "persist.cuh"
 #include "sweep.cuh"
 
 using namespace lddmm;
@@ -72,10 +74,17 @@ struct lddmm_ctx {
   float ow2 = 0.0f;
   int device = 0;
   std::vector<PairDesc> hpd;
-  int NPtot = 0, EDtot = 0, ETtot = 0, ntile_tot = 0, netile_tot = 0, nchunk_tot = 0;
+  int NPtot = 0, EDtot = 0, ETtot = 0, ntile_tot = 0, ngrp_tot = 0, netile_tot = 0,
+      nchunk_tot = 0;
   long long nvar = 0;
   int n_pt_items = 0, n_el_items = 0;
   int S_shoot = 1, S_adj = 1, S_vfd = 1;
+  // persistent multi-step sweeps (one cooperative launch per direction)
+  bool persistent = false;
+  int pers_grid[2] = {0, 0};  // CTAs of the forward / backward persistent kernel
+  int n_units = 0;            // (pair, 8-row group) work units
+  int2 *units = nullptr;
+  StepSync *sync = nullptr;
 
   // device memory
   PairDesc *pd = nullptr;
@@ -83,7 +92,8 @@ struct lddmm_ctx {
   PairState *st = nullptr;
   float4 *qs = nullptr, *as = nullptr, *us = nullptr, *ls = nullptr;
   double *q64 = nullptr, *p64 = nullptr;
-  float4 *ec = nullptr, *en = nullptr, *tc = nullptr, *tn = nullptr;
+  float4 *ec = nullptr, *en = nullptr, *el = nullptr, *tc = nullptr, *tn = nullptr,
+         *tl = nullptr;
   double *e64 = nullptr, *dcdd = nullptr, *tgt64 = nullptr;
   int4 *elm = nullptr;
   int *pt_pair = nullptr, *adj_ptr = nullptr;
@@ -109,6 +119,9 @@ struct lddmm_ctx {
   // dispatch
   cudaError_t (*shoot)(lddmm_ctx &, int t, double *vlc) = nullptr;
   cudaError_t (*adjoint)(lddmm_ctx &, int t, double *g, double *pdot) = nullptr;
+  cudaError_t (*shoot_all)(lddmm_ctx &, double *vlc) = nullptr;
+  cudaError_t (*adjoint_all)(lddmm_ctx &, double *g) = nullptr;
+  int (*pers_blocks)(int which) = nullptr;  // resident CTAs per SM of the persistent kernels
   cudaError_t (*varifold)(lddmm_ctx &) = nullptr;
   cudaError_t (*tt)(lddmm_ctx &, int p, double *part, int nblk, double cw, double dw) = nullptr;
 
@@ -124,33 +137,51 @@ static void dfree(T *&p) {
 lddmm_ctx::~lddmm_ctx() {
   if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
   dfree(pd); dfree(act); dfree(st); dfree(qs); dfree(as); dfree(us); dfree(ls);
-  dfree(q64); dfree(p64); dfree(ec); dfree(en); dfree(tc); dfree(tn); dfree(e64);
+  dfree(q64); dfree(p64); dfree(ec); dfree(en); dfree(el); dfree(tc); dfree(tn); dfree(tl);
+  dfree(e64);
   dfree(dcdd); dfree(tgt64); dfree(elm); dfree(pt_pair); dfree(adj_ptr); dfree(adj);
   dfree(reg_part); dfree(vfd_part); dfree(f_dev); dfree(pt_items); dfree(el_items);
   dfree(chunk_pair); dfree(X); dfree(G); dfree(XT); dfree(GT); dfree(Dv); dfree(Qv);
-  dfree(Sh); dfree(Yh); dfree(part[0]); dfree(part[1]); dfree(rec);
+  dfree(Sh); dfree(Yh); dfree(part[0]); dfree(part[1]); dfree(rec); dfree(sync);
+  dfree(units);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
 // ============================================================ kernel launch
 
+// Every kernel of the objective sweep and the L-BFGS cycle goes through launch():
+// programmatic stream serialisation (the kernel calls pdl_wait() before touching its
+// predecessor's output) and, for the sweeps, the thread-block cluster size.
+template <typename... KArgs, typename... Args>
+static cudaError_t launch(void (*kern)(KArgs...), unsigned grid, unsigned block, int cluster,
+                          cudaStream_t stream, Args &&...args) {
+  if (grid == 0) return cudaSuccess;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[2];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  int na = 1;
+  if (cluster > 0) {
+    attr[1].id = cudaLaunchAttributeClusterDimension;
+    attr[1].val.clusterDim.x = (unsigned)cluster;
+    attr[1].val.clusterDim.y = 1;
+    attr[1].val.clusterDim.z = 1;
+    na = 2;
+  }
+  cfg.attrs = attr;
+  cfg.numAttrs = na;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 template <class Op>
 static cudaError_t launch_sweep(const Op &op, const int2 *items, int n_items, int S,
                                 cudaStream_t stream) {
-  if (n_items == 0) return cudaSuccess;
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(n_items * S));
-  cfg.blockDim = dim3(kWarps * 32);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = stream;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = (unsigned)S;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, sweep_kernel<Op, kWarps>, op, items, S);
+  return launch(sweep_kernel<Op, kWarps>, (unsigned)(n_items * S), kWarps * 32, S, stream, op,
+                items, S);
 }
 
 template <int D, int ORDER>
@@ -189,6 +220,68 @@ static cudaError_t adjoint_impl(lddmm_ctx &c, int t, double *g, double *pdot) {
   return launch_sweep(op, c.pt_items, c.n_pt_items, c.S_adj, c.stream);
 }
 
+// Cooperative launch of a persistent multi-step sweep (all CTAs co-resident; the
+// runtime refuses the launch otherwise).  The barrier counter is reset first.
+template <class Op>
+static cudaError_t launch_persistent(lddmm_ctx &c, const Op &op, int dir, int grid) {
+  CUE(cudaMemsetAsync(&c.sync->arrive, 0, sizeof(unsigned int), c.stream));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3(kPersistWarps * 32);
+  cfg.stream = c.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, persistent_sweep_kernel<Op>, op, (const int2 *)c.units,
+                            c.n_units, c.T, dir, c.sync);
+}
+
+template <int D, int ORDER>
+static cudaError_t shoot_all_impl(lddmm_ctx &c, double *vlc) {
+  ShootOp<D, ORDER> op;
+  op.pd = c.pd;
+  op.act = c.act;
+  op.x64 = c.XT;
+  op.qs0 = c.qs;
+  op.as0 = c.as;
+  op.q640 = c.q64;
+  op.vlc0 = vlc;
+  op.reg0 = c.reg_part;
+  op.NP = c.NPtot;
+  op.ntile = c.ngrp_tot;
+  return launch_persistent(c, op, +1, c.pers_grid[0]);
+}
+
+template <int D, int ORDER>
+static cudaError_t adjoint_all_impl(lddmm_ctx &c, double *g) {
+  AdjointOp<D, ORDER> op;
+  op.pd = c.pd;
+  op.act = c.act;
+  op.p64 = c.p64;
+  op.x64 = c.XT;
+  op.g64 = g;
+  op.pdot64 = nullptr;
+  op.qs0 = c.qs;
+  op.as0 = c.as;
+  op.us0 = c.us;
+  op.ls0 = c.ls;
+  op.NP = c.NPtot;
+  return launch_persistent(c, op, -1, c.pers_grid[1]);
+}
+
+template <int D, int ORDER>
+static int pers_blocks_impl(int which) {
+  int n = 0;
+  cudaError_t e = (which == 0)
+      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, persistent_sweep_kernel<ShootOp<D, ORDER>>, kPersistWarps * 32, 0)
+      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &n, persistent_sweep_kernel<AdjointOp<D, ORDER>>, kPersistWarps * 32, 0);
+  return e == cudaSuccess ? n : 0;
+}
+
 template <int D, char CT, char DT>
 static cudaError_t varifold_impl(lddmm_ctx &c) {
   VarifoldOp<D, CT, DT> op;
@@ -196,8 +289,10 @@ static cudaError_t varifold_impl(lddmm_ctx &c) {
   op.act = c.act;
   op.ec = c.ec;
   op.en = c.en;
+  op.el = c.el;
   op.tc = c.tc;
   op.tn = c.tn;
+  op.tl = c.tl;
   op.e64 = c.e64;
   op.dcdd = c.dcdd;
   op.tile_part = c.vfd_part;
@@ -213,15 +308,24 @@ static cudaError_t tt_impl(lddmm_ctx &c, int p, double *part, int nblk, double c
   return cudaGetLastError();
 }
 
+template <int D, int ORDER>
+static void set_def(lddmm_ctx &c) {
+  c.shoot = shoot_impl<D, ORDER>;
+  c.adjoint = adjoint_impl<D, ORDER>;
+  c.shoot_all = shoot_all_impl<D, ORDER>;
+  c.adjoint_all = adjoint_all_impl<D, ORDER>;
+  c.pers_blocks = pers_blocks_impl<D, ORDER>;
+}
+
 template <int D>
 static bool pick_def(int order, lddmm_ctx &c) {
   switch (order) {
-    case -1: c.shoot = shoot_impl<D, -1>; c.adjoint = adjoint_impl<D, -1>; return true;
-    case 0: if (D == 3) { c.shoot = shoot_impl<D, 0>; c.adjoint = adjoint_impl<D, 0>; return true; } break;
-    case 1: if (D == 3) { c.shoot = shoot_impl<D, 1>; c.adjoint = adjoint_impl<D, 1>; return true; } break;
-    case 2: if (D == 3) { c.shoot = shoot_impl<D, 2>; c.adjoint = adjoint_impl<D, 2>; return true; } break;
-    case 3: if (D == 3) { c.shoot = shoot_impl<D, 3>; c.adjoint = adjoint_impl<D, 3>; return true; } break;
-    case 4: if (D == 3) { c.shoot = shoot_impl<D, 4>; c.adjoint = adjoint_impl<D, 4>; return true; } break;
+    case -1: set_def<D, -1>(c); return true;
+    case 0: if (D == 3) { set_def<D, 0>(c); return true; } break;
+    case 1: if (D == 3) { set_def<D, 1>(c); return true; } break;
+    case 2: if (D == 3) { set_def<D, 2>(c); return true; } break;
+    case 3: if (D == 3) { set_def<D, 3>(c); return true; } break;
+    case 4: if (D == 3) { set_def<D, 4>(c); return true; } break;
   }
   return false;
 }
@@ -244,9 +348,38 @@ static bool pick_vfd(char ct, char dt, lddmm_ctx &c) {
   return false;
 }
 
+// Element geometry at the final positions, the varifold sweep, and the gather that
+// starts the adjoint (us_n/ls_n: operands of the first backward step, or null).
+static cudaError_t launch_geometry(lddmm_ctx &c, const double *q64T) {
+  const unsigned nb = (unsigned)((c.EDtot + 127) / 128);
+  if (c.D == 3)
+    return launch(geometry_kernel<3>, nb, 128, 0, c.stream, c.pd, c.act, c.elm, c.EDtot, q64T,
+                  c.ec, c.en, c.el, c.e64);
+  return launch(geometry_kernel<2>, nb, 128, 0, c.stream, c.pd, c.act, c.elm, c.EDtot, q64T, c.ec,
+                c.en, c.el, c.e64);
+}
+
+static cudaError_t launch_gather(lddmm_ctx &c, const double *q64T, float4 *un, float4 *ln,
+                                 double *dq_out) {
+  const unsigned nb = (unsigned)((c.NPtot + 127) / 128);
+  if (c.D == 3)
+    return launch(gather_kernel<3>, nb, 128, 0, c.stream, c.pd, c.act, c.pt_pair, c.NPtot,
+                  c.adj_ptr, c.adj, c.dcdd, q64T, c.XT, c.p64, un, ln, dq_out, c.T);
+  return launch(gather_kernel<2>, nb, 128, 0, c.stream, c.pd, c.act, c.pt_pair, c.NPtot,
+                c.adj_ptr, c.adj, c.dcdd, q64T, c.XT, c.p64, un, ln, dq_out, c.T);
+}
+
+static cudaError_t launch_objective(lddmm_ctx &c, PairState *st, double *f_out) {
+  const int groups = c.persistent ? kGroup : 0;
+  return launch(objective_kernel, (unsigned)c.P, 128, 0, c.stream, c.pd, c.act, c.reg_part,
+                groups ? c.ngrp_tot : c.ntile_tot, c.vfd_part, c.T, st, f_out, groups);
+}
+
 // FP64 alpha (variable layout) -> FP32 point layout used by the sweeps.
 __global__ void alpha_to_f32_kernel(const PairDesc *__restrict__ pd, int P, const double *x,
                                     float4 *as, int NPtot, int D, int T) {
+  pdl_wait();
+  pdl_trigger();
   const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   // locate the pair (P is small; linear scan)
   int p = 0;
@@ -263,8 +396,14 @@ __global__ void alpha_to_f32_kernel(const PairDesc *__restrict__ pd, int P, cons
 }
 
 __global__ void set_int_kernel(int *a, int n, int v) {
+  pdl_wait();
+  pdl_trigger();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) a[i] = v;
+}
+
+static cudaError_t launch_set_active(lddmm_ctx &c, int n) {
+  return launch(set_int_kernel, (unsigned)((n + 127) / 128), 128, 0, c.stream, c.act, n, 1);
 }
 
 // ==================================================================== setup
@@ -420,6 +559,7 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
     P.el_off = el;
     P.tg_off = tg;
     P.itile_off = it;
+    P.grp_off = it * (kTile / kGroup);
     P.etile_off = et;
     P.var_off = voff;
     P.var_num = (long long)D * a.nde_num * c.T;
@@ -441,6 +581,7 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   c.EDtot = el;
   c.ETtot = tg;
   c.ntile_tot = it;
+  c.ngrp_tot = it * (kTile / kGroup);
   c.netile_tot = et;
   c.nvar = voff;
   c.nchunk_tot = ch;
@@ -460,13 +601,18 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
     for (int k = 0; k < c.hpd[p].Edpad / kTile; ++k) eli.push_back(make_int2(p, k));
   c.n_pt_items = (int)pti.size();
   c.n_el_items = (int)eli.size();
+  std::vector<int2> uni;
+  for (const int2 &x : pti)
+    for (int g = 0; g < kTile / kGroup; ++g)
+      uni.push_back(make_int2(x.x, x.y * (kTile / kGroup) + g));
+  c.n_units = (int)uni.size();
 
   // host-side arrays
   std::vector<float4> h_qs(c.NPtot, make_float4(0, 0, 0, 0));
   std::vector<double> h_q64((size_t)c.NPtot * D, 0.0);
   std::vector<int> h_ptpair(c.NPtot, -1);
   std::vector<int4> h_elm(std::max(c.EDtot, 1), make_int4(0, 0, 0, -1));
-  std::vector<float4> h_tc(std::max(c.ETtot, 1), make_float4(0, 0, 0, 0)), h_tn(h_tc);
+  std::vector<float4> h_tc(std::max(c.ETtot, 1), make_float4(0, 0, 0, 0)), h_tn(h_tc), h_tl(h_tc);
   std::vector<double> h_tgt64((size_t)std::max(c.ETtot, 1) * 8, 0.0);
   std::vector<int> h_adjptr(c.NPtot + 1, 0);
   std::vector<int4> h_adj;
@@ -497,8 +643,14 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
         nn[d] = a.tgt_uni_dir[(size_t)e * D + d];
       }
       const double vol = a.tgt_elm_vol[e];
-      h_tc[g] = make_float4((float)(cc[0] * P.cscale), (float)(cc[1] * P.cscale),
-                            (float)(cc[2] * P.cscale), (float)(-vol));
+      float hi[3], lo[3];
+      for (int d = 0; d < 3; ++d) {
+        const double x = cc[d] * P.cscale;
+        hi[d] = (float)x;
+        lo[d] = (float)(x - (double)hi[d]);
+      }
+      h_tc[g] = make_float4(hi[0], hi[1], hi[2], (float)(-vol));
+      h_tl[g] = make_float4(lo[0], lo[1], lo[2], 0.0f);
       h_tn[g] = make_float4((float)nn[0], (float)nn[1], (float)nn[2], 0.0f);
       double *t8 = &h_tgt64[(size_t)g * 8];
       for (int d = 0; d < 3; ++d) {
@@ -562,8 +714,10 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   CU(dalloc(&c.p64, (size_t)c.NPtot * D));
   CU(dalloc(&c.ec, std::max(c.EDtot, 1)));
   CU(dalloc(&c.en, std::max(c.EDtot, 1)));
+  CU(dalloc(&c.el, std::max(c.EDtot, 1)));
   CU(dalloc(&c.tc, std::max(c.ETtot, 1)));
   CU(dalloc(&c.tn, std::max(c.ETtot, 1)));
+  CU(dalloc(&c.tl, std::max(c.ETtot, 1)));
   CU(dalloc(&c.e64, (size_t)std::max(c.EDtot, 1) * 4));
   CU(dalloc(&c.dcdd, (size_t)std::max(c.EDtot, 1) * 2 * D));
   CU(dalloc(&c.tgt64, h_tgt64.size()));
@@ -571,7 +725,7 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   CU(dalloc(&c.pt_pair, c.NPtot));
   CU(dalloc(&c.adj_ptr, c.NPtot + 1));
   CU(dalloc(&c.adj, std::max<size_t>(h_adj.size(), 1)));
-  CU(dalloc(&c.reg_part, (size_t)c.T * c.ntile_tot));
+  CU(dalloc(&c.reg_part, (size_t)c.T * c.ngrp_tot));
   CU(dalloc(&c.vfd_part, std::max(c.netile_tot, 1)));
   CU(dalloc(&c.f_dev, num));
   CU(dalloc(&c.pt_items, std::max(c.n_pt_items, 1)));
@@ -588,6 +742,7 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   CU(cudaMemcpy(c.elm, h_elm.data(), sizeof(int4) * h_elm.size(), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(c.tc, h_tc.data(), sizeof(float4) * h_tc.size(), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(c.tn, h_tn.data(), sizeof(float4) * h_tn.size(), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(c.tl, h_tl.data(), sizeof(float4) * h_tl.size(), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(c.tgt64, h_tgt64.data(), sizeof(double) * h_tgt64.size(), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(c.adj_ptr, h_adjptr.data(), sizeof(int) * h_adjptr.size(), cudaMemcpyHostToDevice));
   if (!h_adj.empty())
@@ -596,6 +751,8 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
     CU(cudaMemcpy(c.pt_items, pti.data(), sizeof(int2) * pti.size(), cudaMemcpyHostToDevice));
   if (c.n_el_items)
     CU(cudaMemcpy(c.el_items, eli.data(), sizeof(int2) * eli.size(), cudaMemcpyHostToDevice));
+  CU(dalloc(&c.units, std::max(c.n_units, 1)));
+  CU(cudaMemcpy(c.units, uni.data(), sizeof(int2) * uni.size(), cudaMemcpyHostToDevice));
   CU(cudaMemcpy(c.chunk_pair, h_chunk.data(), sizeof(int) * h_chunk.size(), cudaMemcpyHostToDevice));
 
   if (cf.stream) {
@@ -634,11 +791,48 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
       set_err("cluster sizes must be 1, 2, 4 or 8");
       return LDDMM_ERR_ARG;
     }
+  // persistent multi-step sweeps: used when one step of the batch does not fill the
+  // GPU (per-step launches would be latency-bound), sized to the co-resident grid
+  {
+    int sms = 0;
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
+    const int b0 = c.pers_blocks(0), b1 = c.pers_blocks(1);
+    const int cap = std::min(b0, b1) * sms;
+    // automatic: when every row group gets its own resident CTA (one wave) a step is
+    // latency-bound and the persistent sweep wins; bigger batches keep per-step
+    // launches, whose two-rows-per-lane 64-row tiles are cheaper per pair
+    c.persistent = cap > 0 && (cf.persistent > 0 ||
+                               (cf.persistent == 0 && c.n_units <= cap));
+    CU(dalloc(&c.sync, 1));
+    if (c.persistent) {
+      c.pers_grid[0] = std::min(b0 * sms, c.n_units);
+      c.pers_grid[1] = std::min(b1 * sms, c.n_units);
+    }
+  }
   if (cf.autotune) {
     const int rc = autotune(c);
     if (rc) return rc;
   }
   *out = cp.release();
+  return 0;
+}
+
+// Clears the persistent sweeps' barrier and error words (start of every entry point).
+static cudaError_t reset_sync(lddmm_ctx &c) {
+  return cudaMemsetAsync(c.sync, 0, 2 * sizeof(unsigned int), c.stream);
+}
+
+// LDDMM_ERR_TIMEOUT when a persistent sweep's grid barrier gave up (stream must be
+// synchronised by the caller).
+static int check_sync(lddmm_ctx &c) {
+  if (!c.persistent) return 0;
+  unsigned int w[2] = {0, 0};
+  CU(cudaMemcpy(w, c.sync, sizeof(w), cudaMemcpyDeviceToHost));
+  if (w[1]) {
+    set_err("a persistent sweep's grid barrier timed out at step %u (the grid was not "
+            "co-resident)", w[1] - 1);
+    return LDDMM_ERR_TIMEOUT;
+  }
   return 0;
 }
 
@@ -671,35 +865,27 @@ extern "C" int lddmm_ctx_launch_config(const lddmm_ctx *c, int *o) {
 static cudaError_t run_eval(lddmm_ctx &c, double *g_out, double *f_out, double *vlc,
                             bool grad) {
   const int D = c.D;
-  for (int t = 0; t < c.T; ++t)
-    CUE(c.shoot(c, t, vlc ? vlc + (size_t)t * c.NPtot * D : nullptr));
+  if (c.persistent) {
+    CUE(c.shoot_all(c, vlc));
+  } else {
+    for (int t = 0; t < c.T; ++t)
+      CUE(c.shoot(c, t, vlc ? vlc + (size_t)t * c.NPtot * D : nullptr));
+  }
   const double *q64T = c.q64 + (size_t)c.T * c.NPtot * D;
   if (c.has_vfd) {
-    const int nb = (c.EDtot + 127) / 128;
-    if (D == 3)
-      geometry_kernel<3><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
-    else
-      geometry_kernel<2><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
-    CUE(cudaGetLastError());
+    CUE(launch_geometry(c, q64T));
     CUE(c.varifold(c));
   }
-  if (grad) {
-    const int nb = (c.NPtot + 127) / 128;
-    float4 *un = c.us + (size_t)((c.T - 1) & 1) * c.NPtot;
-    float4 *ln = c.ls + (size_t)((c.T - 1) & 1) * c.NPtot;
-    if (D == 3)
-      gather_kernel<3><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
-                                                  c.dcdd, q64T, c.XT, c.p64, un, ln, nullptr, c.T);
-    else
-      gather_kernel<2><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
-                                                  c.dcdd, q64T, c.XT, c.p64, un, ln, nullptr, c.T);
-    CUE(cudaGetLastError());
-  }
-  objective_kernel<<<c.P, 128, 0, c.stream>>>(c.pd, c.act, c.reg_part, c.ntile_tot, c.vfd_part,
-                                               c.T, c.st, f_out);
-  CUE(cudaGetLastError());
   if (grad)
-    for (int t = c.T - 1; t >= 0; --t) CUE(c.adjoint(c, t, g_out, nullptr));
+    CUE(launch_gather(c, q64T, c.us + (size_t)((c.T - 1) & 1) * c.NPtot,
+                      c.ls + (size_t)((c.T - 1) & 1) * c.NPtot, nullptr));
+  CUE(launch_objective(c, c.st, f_out));
+  if (grad) {
+    if (c.persistent)
+      CUE(c.adjoint_all(c, g_out));
+    else
+      for (int t = c.T - 1; t >= 0; --t) CUE(c.adjoint(c, t, g_out, nullptr));
+  }
   return cudaSuccess;
 }
 
@@ -707,9 +893,8 @@ static cudaError_t load_trial(lddmm_ctx &c, const double *d_alp, bool host) {
   CUE(cudaMemcpyAsync(c.XT, d_alp, sizeof(double) * c.nvar,
                       host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, c.stream));
   const long long n = c.nvar;
-  alpha_to_f32_kernel<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(c.pd, c.P, c.XT, c.as,
-                                                                          c.NPtot, c.D, c.T);
-  return cudaGetLastError();
+  return launch(alpha_to_f32_kernel, (unsigned)((n + 255) / 256), 256, 0, c.stream, c.pd, c.P,
+                (const double *)c.XT, c.as, c.NPtot, c.D, c.T);
 }
 
 extern "C" int lddmm_objgrd_device(lddmm_ctx *ctx, const double *d_alp, double *d_fcn,
@@ -720,11 +905,14 @@ extern "C" int lddmm_objgrd_device(lddmm_ctx *ctx, const double *d_alp, double *
   }
   lddmm_ctx &c = *ctx;
   CU(cudaSetDevice(c.device));
-  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
-  CU(cudaGetLastError());
+  CU(reset_sync(c));
+  CU(launch_set_active(c, c.P));
   CU(load_trial(c, d_alp, false));
   CU(run_eval(c, d_grd ? d_grd : c.GT, d_fcn, nullptr, true));
-  if (!async) CU(cudaStreamSynchronize(c.stream));
+  if (!async) {
+    CU(cudaStreamSynchronize(c.stream));
+    return check_sync(c);
+  }
   return 0;
 }
 
@@ -735,14 +923,14 @@ extern "C" int lddmm_objgrd(lddmm_ctx *ctx, const double *alp, double *fcn, doub
   }
   lddmm_ctx &c = *ctx;
   CU(cudaSetDevice(c.device));
-  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
-  CU(cudaGetLastError());
+  CU(reset_sync(c));
+  CU(launch_set_active(c, c.P));
   CU(load_trial(c, alp, true));
   CU(run_eval(c, c.GT, c.f_dev, nullptr, grd != nullptr));
   CU(cudaMemcpyAsync(fcn, c.f_dev, sizeof(double) * c.P, cudaMemcpyDeviceToHost, c.stream));
   if (grd) CU(cudaMemcpyAsync(grd, c.GT, sizeof(double) * c.nvar, cudaMemcpyDeviceToHost, c.stream));
   CU(cudaStreamSynchronize(c.stream));
-  return 0;
+  return check_sync(c);
 }
 
 extern "C" int lddmm_shoot(lddmm_ctx *ctx, const double *alp, double *nde_stk, double *vlc_stk) {
@@ -753,12 +941,13 @@ extern "C" int lddmm_shoot(lddmm_ctx *ctx, const double *alp, double *nde_stk, d
   lddmm_ctx &c = *ctx;
   const int D = c.D;
   CU(cudaSetDevice(c.device));
-  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
+  CU(launch_set_active(c, c.P));
   CU(load_trial(c, alp, true));
   double *vlc = nullptr;
   CU(dalloc(&vlc, (size_t)c.T * c.NPtot * D));
-  cudaError_t e = cudaSuccess;
-  for (int t = 0; t < c.T && e == cudaSuccess; ++t)
+  cudaError_t e = reset_sync(c);
+  if (e == cudaSuccess && c.persistent) e = c.shoot_all(c, vlc);
+  for (int t = 0; t < c.T && e == cudaSuccess && !c.persistent; ++t)
     e = c.shoot(c, t, vlc + (size_t)t * c.NPtot * D);
   std::vector<double> hq((size_t)(c.T + 1) * c.NPtot * D), hv((size_t)c.T * c.NPtot * D);
   if (e == cudaSuccess)
@@ -768,6 +957,10 @@ extern "C" int lddmm_shoot(lddmm_ctx *ctx, const double *alp, double *nde_stk, d
   if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
   cudaFree(vlc);
   CU(e);
+  {
+    const int rc = check_sync(c);
+    if (rc) return rc;
+  }
   // un-pad: per pair, time-major blocks of N x D
   size_t on = 0, ov = 0;
   for (int p = 0; p < c.P; ++p) {
@@ -832,19 +1025,19 @@ static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o) {
   auto pass = [&](int mode, int k) -> cudaError_t {
     A.part_out = c.part[s & 1];
     A.part_in = c.part[(s + 1) & 1];
-    vec_pass_kernel<<<nb, kVecThreads, 0, c.stream>>>(A, mode, k);
+    const cudaError_t e = launch(vec_pass_kernel, nb, kVecThreads, 0, c.stream, A, mode, k);
     ++s;
-    return cudaGetLastError();
+    return e;
   };
   CUE(pass(kPost, 0));
-  decide_kernel<<<pb, 128, 0, c.stream>>>(c.pd, c.st, c.P, c.part[0], o, c.rec);
-  CUE(cudaGetLastError());
+  CUE(launch(decide_kernel, (unsigned)pb, 128, 0, c.stream, (const PairDesc *)c.pd, c.st, c.P,
+             (const double *)c.part[0], o, c.rec));
   CUE(pass(kAccept, 0));
   for (int k = 0; k < o.mem_num; ++k) CUE(pass(kTwoLoopB, k));
   for (int k = 0; k < o.mem_num; ++k) CUE(pass(kTwoLoopF, k));
   CUE(pass(kFin, 0));
-  ls_init_kernel<<<pb, 128, 0, c.stream>>>(c.pd, c.st, c.P, c.part[(s - 1) & 1], c.act);
-  return cudaGetLastError();
+  return launch(ls_init_kernel, (unsigned)pb, 128, 0, c.stream, (const PairDesc *)c.pd, c.st, c.P,
+                (const double *)c.part[(s - 1) & 1], c.act);
 }
 
 static long long kernels_per_cycle(const lddmm_ctx &c, int m) {
@@ -922,8 +1115,7 @@ static int lbfgs_run(lddmm_ctx &c, const lddmm_opt *opt, const double *alp, bool
     s.newIdx = -1;
   }
   CU(cudaMemcpyAsync(c.st, hs.data(), sizeof(PairState) * c.P, cudaMemcpyHostToDevice, c.stream));
-  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
-  CU(cudaGetLastError());
+  CU(launch_set_active(c, c.P));
   CU(load_trial(c, alp, host));
   CU(cudaMemcpyAsync(c.X, c.XT, sizeof(double) * c.nvar, cudaMemcpyDeviceToDevice, c.stream));
   if (c.use_graph) {
@@ -947,6 +1139,10 @@ static int lbfgs_run(lddmm_ctx &c, const lddmm_opt *opt, const double *alp, bool
     cycles += check_every;
     CU(cudaMemcpyAsync(hact.data(), c.act, sizeof(int) * c.P, cudaMemcpyDeviceToHost, c.stream));
     CU(cudaStreamSynchronize(c.stream));
+    {
+      const int rc = check_sync(c);
+      if (rc) return rc;
+    }
     bool any = false;
     for (int a : hact) any |= (a != 0);
     if (!any) break;
@@ -1031,8 +1227,7 @@ extern "C" int lddmm_ctx_time_sweeps(lddmm_ctx *ctx, int reps, double *ms4) {
   if (!ctx || reps <= 0 || !ms4) return LDDMM_ERR_ARG;
   lddmm_ctx &c = *ctx;
   CU(cudaSetDevice(c.device));
-  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
-  CU(cudaGetLastError());
+  CU(launch_set_active(c, c.P));
   const int nev = 2 * c.T + 1;
   std::vector<cudaEvent_t> ev(2 * nev + 2);
   for (auto &e : ev) CU(cudaEventCreate(&e));
@@ -1040,51 +1235,63 @@ extern "C" int lddmm_ctx_time_sweeps(lddmm_ctx *ctx, int reps, double *ms4) {
   int cnt[3] = {0, 0, 0};
   const int D = c.D;
   cudaError_t err = cudaSuccess;
+  CU(reset_sync(c));
   for (int r = 0; r < reps && err == cudaSuccess; ++r) {
     cudaEventRecord(ev[2 * nev], c.stream);
-    for (int t = 0; t < c.T; ++t) {
-      cudaEventRecord(ev[2 * t], c.stream);
-      err = c.shoot(c, t, nullptr);
-      cudaEventRecord(ev[2 * t + 1], c.stream);
+    if (c.persistent) {
+      cudaEventRecord(ev[0], c.stream);
+      err = c.shoot_all(c, nullptr);
+      cudaEventRecord(ev[1], c.stream);
+    } else {
+      for (int t = 0; t < c.T; ++t) {
+        cudaEventRecord(ev[2 * t], c.stream);
+        if (err == cudaSuccess) err = c.shoot(c, t, nullptr);
+        cudaEventRecord(ev[2 * t + 1], c.stream);
+      }
     }
     const double *q64T = c.q64 + (size_t)c.T * c.NPtot * D;
     if (c.has_vfd) {
-      const int nb = (c.EDtot + 127) / 128;
-      if (D == 3)
-        geometry_kernel<3><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
-      else
-        geometry_kernel<2><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
+      if (err == cudaSuccess) err = launch_geometry(c, q64T);
       cudaEventRecord(ev[4 * c.T], c.stream);
       if (err == cudaSuccess) err = c.varifold(c);
       cudaEventRecord(ev[4 * c.T + 1], c.stream);
     }
-    const int nb = (c.NPtot + 127) / 128;
-    float4 *un = c.us + (size_t)((c.T - 1) & 1) * c.NPtot;
-    float4 *ln = c.ls + (size_t)((c.T - 1) & 1) * c.NPtot;
-    if (D == 3)
-      gather_kernel<3><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
-                                                  c.dcdd, q64T, c.XT, c.p64, un, ln, nullptr, c.T);
-    else
-      gather_kernel<2><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
-                                                  c.dcdd, q64T, c.XT, c.p64, un, ln, nullptr, c.T);
-    objective_kernel<<<c.P, 128, 0, c.stream>>>(c.pd, c.act, c.reg_part, c.ntile_tot, c.vfd_part,
-                                                 c.T, nullptr, c.f_dev);
-    for (int t = c.T - 1; t >= 0 && err == cudaSuccess; --t) {
-      cudaEventRecord(ev[2 * c.T + 2 * t], c.stream);
-      err = c.adjoint(c, t, c.GT, nullptr);
-      cudaEventRecord(ev[2 * c.T + 2 * t + 1], c.stream);
+    if (err == cudaSuccess)
+      err = launch_gather(c, q64T, c.us + (size_t)((c.T - 1) & 1) * c.NPtot,
+                          c.ls + (size_t)((c.T - 1) & 1) * c.NPtot, nullptr);
+    if (err == cudaSuccess) err = launch_objective(c, nullptr, c.f_dev);
+    if (c.persistent) {
+      cudaEventRecord(ev[2 * c.T], c.stream);
+      if (err == cudaSuccess) err = c.adjoint_all(c, c.GT);
+      cudaEventRecord(ev[2 * c.T + 1], c.stream);
+    } else {
+      for (int t = c.T - 1; t >= 0 && err == cudaSuccess; --t) {
+        cudaEventRecord(ev[2 * c.T + 2 * t], c.stream);
+        err = c.adjoint(c, t, c.GT, nullptr);
+        cudaEventRecord(ev[2 * c.T + 2 * t + 1], c.stream);
+      }
     }
     cudaEventRecord(ev[2 * nev + 1], c.stream);
     if (err == cudaSuccess) err = cudaEventSynchronize(ev[2 * nev + 1]);
     if (err != cudaSuccess) break;
     float ms = 0.0f;
-    for (int t = 0; t < c.T; ++t) {
-      cudaEventElapsedTime(&ms, ev[2 * t], ev[2 * t + 1]);
-      acc[0] += ms;
+    if (c.persistent) {
+      // one launch covers all T steps: report the per-step share
+      cudaEventElapsedTime(&ms, ev[0], ev[1]);
+      acc[0] += ms / c.T;
       cnt[0]++;
-      cudaEventElapsedTime(&ms, ev[2 * c.T + 2 * t], ev[2 * c.T + 2 * t + 1]);
-      acc[1] += ms;
+      cudaEventElapsedTime(&ms, ev[2 * c.T], ev[2 * c.T + 1]);
+      acc[1] += ms / c.T;
       cnt[1]++;
+    } else {
+      for (int t = 0; t < c.T; ++t) {
+        cudaEventElapsedTime(&ms, ev[2 * t], ev[2 * t + 1]);
+        acc[0] += ms;
+        cnt[0]++;
+        cudaEventElapsedTime(&ms, ev[2 * c.T + 2 * t], ev[2 * c.T + 2 * t + 1]);
+        acc[1] += ms;
+        cnt[1]++;
+      }
     }
     if (c.has_vfd) {
       cudaEventElapsedTime(&ms, ev[4 * c.T], ev[4 * c.T + 1]);
@@ -1108,8 +1315,7 @@ extern "C" int lddmm_ctx_time_sweeps(lddmm_ctx *ctx, int reps, double *ms4) {
 static int autotune(lddmm_ctx &c) {
   // Time every cluster size for each sweep on this batch (zero momenta; the cost
   // does not depend on the values) and keep the fastest.
-  set_int_kernel<<<(c.P + 127) / 128, 128, 0, c.stream>>>(c.act, c.P, 1);
-  CU(cudaGetLastError());
+  CU(launch_set_active(c, c.P));
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
@@ -1219,7 +1425,7 @@ extern "C" int lddmm_dq_kernel(int dim, int n, const double *q, const double *l,
   CU(cudaMemsetAsync(c.us, 0, sizeof(float4) * c.NPtot, c.stream));
   CU(cudaMemcpyAsync(c.ls, hl.data(), sizeof(float4) * c.NPtot, cudaMemcpyHostToDevice, c.stream));
   CU(cudaMemcpyAsync(c.as, hr.data(), sizeof(float4) * c.NPtot, cudaMemcpyHostToDevice, c.stream));
-  set_int_kernel<<<1, 32, 0, c.stream>>>(c.act, 1, 1);
+  CU(launch_set_active(c, 1));
   CU(c.adjoint(c, 0, nullptr, pd));
   std::vector<double> h((size_t)c.NPtot * dim);
   CU(cudaMemcpyAsync(h.data(), pd, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c.stream));
@@ -1252,31 +1458,17 @@ extern "C" int lddmm_varifold(const lddmm_problem *prob, const double *nde, doub
   // positions at the final time = nde; zero energy partials
   double *q64T = c.q64 + (size_t)c.T * c.NPtot * D;
   CU(cudaMemcpyAsync(q64T, c.q64, sizeof(double) * c.NPtot * D, cudaMemcpyDeviceToDevice, c.stream));
-  CU(cudaMemsetAsync(c.reg_part, 0, sizeof(double) * c.T * c.ntile_tot, c.stream));
-  set_int_kernel<<<1, 32, 0, c.stream>>>(c.act, 1, 1);
+  CU(cudaMemsetAsync(c.reg_part, 0, sizeof(double) * c.T * c.ngrp_tot, c.stream));
+  CU(launch_set_active(c, 1));
   double *dqd = nullptr;
   CU(dalloc(&dqd, (size_t)c.NPtot * D));
   std::unique_ptr<double, cudaError_t (*)(void *)> g2(dqd, cudaFree);
   if (c.has_vfd) {
-    const int nb = (c.EDtot + 127) / 128;
-    if (D == 3)
-      geometry_kernel<3><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
-    else
-      geometry_kernel<2><<<nb, 128, 0, c.stream>>>(c.pd, c.act, c.elm, c.EDtot, q64T, c.ec, c.en, c.e64);
-    CU(cudaGetLastError());
+    CU(launch_geometry(c, q64T));
     CU(c.varifold(c));
-    const int np = (c.NPtot + 127) / 128;
-    if (D == 3)
-      gather_kernel<3><<<np, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
-                                                  c.dcdd, q64T, c.XT, c.p64, nullptr, nullptr, dqd, c.T);
-    else
-      gather_kernel<2><<<np, 128, 0, c.stream>>>(c.pd, c.act, c.pt_pair, c.NPtot, c.adj_ptr, c.adj,
-                                                  c.dcdd, q64T, c.XT, c.p64, nullptr, nullptr, dqd, c.T);
-    CU(cudaGetLastError());
+    CU(launch_gather(c, q64T, nullptr, nullptr, dqd));
   }
-  objective_kernel<<<1, 128, 0, c.stream>>>(c.pd, c.act, c.reg_part, c.ntile_tot, c.vfd_part, c.T,
-                                             nullptr, c.f_dev);
-  CU(cudaGetLastError());
+  CU(launch_objective(c, nullptr, c.f_dev));
   std::vector<double> h((size_t)c.NPtot * D);
   CU(cudaMemcpyAsync(val, c.f_dev, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   CU(cudaMemcpyAsync(h.data(), dqd, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c.stream));

@@ -36,20 +36,35 @@ struct ShootOp {
   double *vlc64;       // optional velocity output       [NPtot * D]
   double *tile_part;   // energy partial per i-tile of this step
   int t;
+  // bases for the persistent multi-step sweep (set_step derives the fields above)
+  const float4 *qs0, *as0;
+  double *q640, *vlc0, *reg0;
+  int NP, ntile;  // ntile: stride of reg0 per step (row groups in the persistent sweep)
+
+  __device__ void set_step(int tt) {
+    t = tt;
+    qs_t = qs0 + (size_t)tt * NP;
+    as_t = as0 + (size_t)tt * NP;
+    q64_t = q640 + (size_t)tt * NP * D;
+    q64_n = q640 + (size_t)(tt + 1) * NP * D;
+    qs_n = const_cast<float4 *>(qs0) + (size_t)(tt + 1) * NP;
+    vlc64 = vlc0 ? vlc0 + (size_t)tt * NP * D : nullptr;
+    tile_part = reg0 + (size_t)tt * ntile;
+  }
 
   __device__ bool active(int p) const { return act[p] != 0; }
   __device__ int j_count(int p) const { return pd[p].Npad; }
-  __device__ int j_set(int, int) const { return 0; }
+  __device__ int set_boundary(int p) const { return pd[p].Npad; }
   __device__ void load_i(int p, int row, IData &I) const {
-    const float4 q = qs_t[pd[p].pt_off + row];
+    const float4 q = __ldcg(&qs_t[pd[p].pt_off + row]);
     I.x = q.x;
     I.y = q.y;
     I.z = q.z;
   }
   __device__ void load_j(int p, int j, float4 (&w)[JW]) const {
     const int g = pd[p].pt_off + j;
-    w[0] = __ldg(&qs_t[g]);
-    w[1] = __ldg(&as_t[g]);
+    w[0] = __ldcg(&qs_t[g]);
+    w[1] = __ldcg(&as_t[g]);
   }
   template <int SET>
   __device__ __forceinline__ void pair(const IData &I, const float4 (&w)[JW],
@@ -86,6 +101,9 @@ struct ShootOp {
   __device__ void write_tile(int p, int tile, double v) const {
     tile_part[pd[p].itile_off + tile] = v;
   }
+  __device__ void write_group(int p, int grp, double v) const {
+    tile_part[pd[p].grp_off + grp] = v;
+  }
 };
 
 // ------------------------------------------------------------------ backward
@@ -115,13 +133,27 @@ struct AdjointOp {
   float4 *ls_n;        // l_{t-1}
   double *pdot64;      // optional raw dq output [NPtot * D] (standalone dq kernel)
   int t;
+  // bases for the persistent multi-step sweep
+  const float4 *qs0, *as0;
+  float4 *us0, *ls0;
+  int NP;
+
+  __device__ void set_step(int tt) {
+    t = tt;
+    qs_t = qs0 + (size_t)tt * NP;
+    as_t = as0 + (size_t)tt * NP;
+    us_t = us0 + (size_t)(tt & 1) * NP;
+    ls_t = ls0 + (size_t)(tt & 1) * NP;
+    us_n = tt > 0 ? us0 + (size_t)((tt - 1) & 1) * NP : nullptr;
+    ls_n = tt > 0 ? ls0 + (size_t)((tt - 1) & 1) * NP : nullptr;
+  }
 
   __device__ bool active(int p) const { return act[p] != 0; }
   __device__ int j_count(int p) const { return pd[p].Npad; }
-  __device__ int j_set(int, int) const { return 0; }
+  __device__ int set_boundary(int p) const { return pd[p].Npad; }
   __device__ void load_i(int p, int row, IData &I) const {
     const int g = pd[p].pt_off + row;
-    const float4 q = qs_t[g], l = ls_t[g], r = as_t[g];
+    const float4 q = __ldcg(&qs_t[g]), l = __ldcg(&ls_t[g]), r = __ldcg(&as_t[g]);
     I.q[0] = q.x; I.q[1] = q.y;
     I.l[0] = l.x; I.l[1] = l.y;
     I.r[0] = r.x; I.r[1] = r.y;
@@ -133,8 +165,8 @@ struct AdjointOp {
   }
   __device__ void load_j(int p, int j, float4 (&w)[JW]) const {
     const int g = pd[p].pt_off + j;
-    const float4 q = __ldg(&qs_t[g]), u = __ldg(&us_t[g]), l = __ldg(&ls_t[g]),
-                 r = __ldg(&as_t[g]);
+    const float4 q = __ldcg(&qs_t[g]), u = __ldcg(&us_t[g]), l = __ldcg(&ls_t[g]),
+                 r = __ldcg(&as_t[g]);
     if (D == 3) {
       w[0] = make_float4(q.x, q.y, q.z, u.x);
       w[1] = make_float4(u.y, u.z, l.x, l.y);
@@ -207,6 +239,7 @@ struct AdjointOp {
     return 0.0;
   }
   __device__ void write_tile(int, int, double) const {}
+  __device__ void write_group(int, int, double) const {}
 };
 
 // ------------------------------------------------------------------ varifold
@@ -219,23 +252,31 @@ struct AdjointOp {
 // Cpp/src/varifold2D.cpp:245-310) with grassmanFunction's derivative expanded: for
 // the unnormalised normal N (|N| = 2 a_i in 3D, a_i in 2D) its 1/|N| cancels the
 // a_i / (2 a_i) and the area derivative 0.5 n (3D) / n (2D).
-// j data: (c_scaled.xyz, w) (n.xyz, 0);  2D: (cx cy 0 w) (nx ny 0 0).
+//
+// Centres are carried as double-single pairs (hi + lo, both FP32) so the centre
+// difference (hi_i - hi_j) + (lo_i - lo_j) is accurate to an ulp of the difference
+// itself: near convergence V and dV/dq are small differences of the DD and DT sums,
+// and a plain FP32 rounding of the centres (relative 1e-6 on neighbour distances)
+// would dominate their error.
+// j data, 3D: (chi.xyz, w) (n.xyz, clo.x) (clo.y, clo.z, -, -)
+//         2D: (chi.xy, clo.xy) (n.xy, w, -)
 // Accumulators: 0 S_DD, 1 S_DT, 2.. A (D), 2+D.. C (D), [2+2D B for non-Binet].
 
 template <int D, char CT, char DT>
 struct VarifoldOp {
   static constexpr bool kBinet = (DT == 'B');
-  static constexpr int JW = 2;
+  static constexpr int JW = (D == 3) ? 3 : 2;
   static constexpr int NA = 2 + 2 * D + (kBinet ? 0 : 1);
   static constexpr bool kTileSum = true;
   static constexpr bool kTwoSets = true;
   struct IData {
-    float c[D], n[D];
+    float ch[D], cl[D], n[D];
   };
   const PairDesc *pd;
   const int *act;
-  const float4 *ec, *en;  // deformed: scaled centre + area, unit normal
-  const float4 *tc, *tn;  // target:   scaled centre - area, unit normal
+  const float4 *ec, *en;  // deformed: scaled centre hi + area, normal + centre lo.x
+  const float4 *el;       // deformed: centre lo (xyz)
+  const float4 *tc, *tn, *tl;  // target: same with weight -area
   const double *e64;      // deformed (n.xyz, area) FP64              [EDtot * 4]
   double *dcdd;           // out: dc (D), dd (D) per deformed element [EDtot * 2D]
   double *tile_part;      // varifold value per element tile
@@ -243,43 +284,64 @@ struct VarifoldOp {
 
   __device__ bool active(int p) const { return act[p] != 0; }
   __device__ int j_count(int p) const { return pd[p].Edpad + pd[p].Etpad; }
-  __device__ int j_set(int p, int j0) const { return j0 >= pd[p].Edpad ? 1 : 0; }
+  __device__ int set_boundary(int p) const { return pd[p].Edpad; }
   __device__ void load_i(int p, int row, IData &I) const {
     const int g = pd[p].el_off + row;
-    const float4 c = ec[g], n = en[g];
-    I.c[0] = c.x; I.c[1] = c.y;
+    const float4 c = ec[g], n = en[g], l = el[g];
+    I.ch[0] = c.x; I.ch[1] = c.y;
+    I.cl[0] = l.x; I.cl[1] = l.y;
     I.n[0] = n.x; I.n[1] = n.y;
     if (D == 3) {
-      I.c[D - 1] = c.z;
+      I.ch[D - 1] = c.z;
+      I.cl[D - 1] = l.z;
       I.n[D - 1] = n.z;
     }
   }
   __device__ void load_j(int p, int j, float4 (&w)[JW]) const {
     const PairDesc &P = pd[p];
+    float4 c, n, l;
     if (j < P.Edpad) {
-      w[0] = __ldg(&ec[P.el_off + j]);
-      w[1] = __ldg(&en[P.el_off + j]);
+      c = __ldcg(&ec[P.el_off + j]);
+      n = __ldcg(&en[P.el_off + j]);
+      l = __ldcg(&el[P.el_off + j]);
     } else {
-      w[0] = __ldg(&tc[P.tg_off + j - P.Edpad]);
-      w[1] = __ldg(&tn[P.tg_off + j - P.Edpad]);
+      c = __ldcg(&tc[P.tg_off + j - P.Edpad]);
+      n = __ldcg(&tn[P.tg_off + j - P.Edpad]);
+      l = __ldcg(&tl[P.tg_off + j - P.Edpad]);
+    }
+    if (D == 3) {
+      w[0] = c;
+      w[1] = make_float4(n.x, n.y, n.z, l.x);
+      w[JW - 1] = make_float4(l.y, l.z, 0.0f, 0.0f);
+    } else {
+      w[0] = make_float4(c.x, c.y, l.x, l.y);
+      w[1] = make_float4(n.x, n.y, c.w, 0.0f);
     }
   }
   template <int SET>
   __device__ __forceinline__ void pair(const IData &I, const float4 (&w)[JW],
                                        float (&acc)[NA]) const {
-    const float cj[3] = {w[0].x, w[0].y, w[0].z};
-    const float nj[3] = {w[1].x, w[1].y, w[1].z};
+    float chj[3], clj[3], nj[3], wt;
+    if (D == 3) {
+      chj[0] = w[0].x; chj[1] = w[0].y; chj[2] = w[0].z; wt = w[0].w;
+      nj[0] = w[1].x; nj[1] = w[1].y; nj[2] = w[1].z;
+      clj[0] = w[1].w; clj[1] = w[JW - 1].x; clj[2] = w[JW - 1].y;
+    } else {
+      chj[0] = w[0].x; chj[1] = w[0].y; clj[0] = w[0].z; clj[1] = w[0].w;
+      nj[0] = w[1].x; nj[1] = w[1].y; wt = w[1].z;
+      chj[2] = clj[2] = nj[2] = 0.0f;
+    }
     float dc[D];
     float nr2 = 0.0f, ang = 0.0f;
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-      dc[d] = I.c[d] - cj[d];
+      dc[d] = (I.ch[d] - chj[d]) + (I.cl[d] - clj[d]);
       nr2 = fmaf(-dc[d], dc[d], nr2);
       ang = fmaf(I.n[d], nj[d], ang);
     }
     float k, kg;
     CenKernel<CT>::val_w(nr2, k, kg);
-    const float kw = k * w[0].w;
+    const float kw = k * wt;
     if (kBinet) {
       const float t1 = kw * ang;  // k w b'/2
       const float tb = t1 * ang;  // k w b
@@ -342,7 +404,9 @@ template <int D>
 __global__ void geometry_kernel(const PairDesc *__restrict__ pd, const int *__restrict__ act,
                                 const int4 *__restrict__ elm, int n_elm,
                                 const double *__restrict__ q64, float4 *ec, float4 *en,
-                                double *e64) {
+                                float4 *el, double *e64) {
+  pdl_wait();
+  pdl_trigger();
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n_elm) return;
   const int4 ev = elm[g];
@@ -376,8 +440,15 @@ __global__ void geometry_kernel(const PairDesc *__restrict__ pd, const int *__re
     a = len;
   }
   const double s = P.cscale;
-  ec[g] = make_float4((float)(c[0] * s), (float)(c[1] * s), (float)(c[2] * s), (float)a);
+  float hi[3], lo[3];
+  for (int d = 0; d < 3; ++d) {
+    const double x = c[d] * s;
+    hi[d] = (float)x;
+    lo[d] = (float)(x - (double)hi[d]);
+  }
+  ec[g] = make_float4(hi[0], hi[1], hi[2], (float)a);
   en[g] = make_float4((float)n[0], (float)n[1], (float)n[2], 0.0f);
+  el[g] = make_float4(lo[0], lo[1], lo[2], 0.0f);
   double *e = e64 + (size_t)g * 4;
   e[0] = n[0];
   e[1] = n[1];
@@ -395,6 +466,8 @@ __global__ void gather_kernel(const PairDesc *__restrict__ pd, const int *__rest
                               const double *__restrict__ dcdd, const double *__restrict__ q64T,
                               const double *__restrict__ x64, double *p64, float4 *us_n,
                               float4 *ls_n, double *dq_out, int T) {
+  pdl_wait();
+  pdl_trigger();
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n_pt) return;
   const int p = pt_pair[g];
@@ -440,19 +513,24 @@ __global__ void gather_kernel(const PairDesc *__restrict__ pd, const int *__rest
 
 // E = dt/2 sum_t a_t.v_t + w (V_DD,DT + V_TT)   (Cpp/src/objgrd.cpp:65).  One CTA
 // per pair, partials summed in fixed order.
+// reg_part holds one energy partial per (time step, row block): 64-row i-tiles after
+// per-step sweeps (groups = 0), `groups`-row groups after persistent sweeps.
 __global__ void objective_kernel(const PairDesc *__restrict__ pd, const int *__restrict__ act,
                                  const double *__restrict__ reg_part, int ntile_tot,
                                  const double *__restrict__ vfd_part, int T, PairState *st,
-                                 double *f_out) {
+                                 double *f_out, int groups) {
   __shared__ double scr[32];
+  pdl_wait();
+  pdl_trigger();
   const int p = blockIdx.x;
   if (!act[p]) return;
   const PairDesc &P = pd[p];
-  const int nt = P.Npad / kTile, ne = P.Edpad / kTile;
+  const int nt = P.Npad / (groups > 0 ? groups : kTile), ne = P.Edpad / kTile;
+  const int off = groups ? P.grp_off : P.itile_off;
   double r = 0.0, v = 0.0;
   for (int k = threadIdx.x; k < T * nt; k += blockDim.x) {
     const int t = k / nt, i = k - t * nt;
-    r += reg_part[(size_t)t * ntile_tot + P.itile_off + i];
+    r += reg_part[(size_t)t * ntile_tot + off + i];
   }
   for (int k = threadIdx.x; k < ne; k += blockDim.x) v += vfd_part[P.etile_off + k];
   const double R = block_sum(r, scr);

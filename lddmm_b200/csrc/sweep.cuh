@@ -3,12 +3,13 @@
 // Work decomposition (one launch per sweep, every pair of the batch in it):
 //   item    = (pair, i-tile of kTile = 64 rows); the item list is built on the host,
 //             largest pairs first.
-//   cluster = S CTAs on one item (thread-block cluster along x); CTA rank r takes
-//             every S-th group of W j-sub-tiles.
+//   cluster = S CTAs on one item (thread-block cluster along x); the S x W warps of
+//             the cluster split the item's j range into contiguous shares that differ
+//             by at most one point.
 //   CTA     = W warps; every warp owns all 64 rows of the tile (2 rows per lane) and
-//             its own 32-point j-sub-tiles, staged warp-privately in shared memory
-//             with the next sub-tile prefetched into registers, so warps never wait
-//             on each other inside the j loop.
+//             walks its share in 32-point sub-tiles, staged warp-privately in shared
+//             memory with the next sub-tile prefetched into registers, so warps never
+//             wait on each other inside the j loop.
 // Each 32-pair sub-tile is summed in plain FP32 and folded into a (hi, lo) TwoSum
 // accumulator.  Warps are combined in FP64 through shared memory, the cluster's
 // CTAs through distributed shared memory (DSMEM) in fixed rank order, so every
@@ -21,9 +22,9 @@
 //   active(p)         evaluate pair p in this sweep
 //   load_i(p, row, I) load row data
 //   j_count(p)        padded j extent (multiple of kTile)
-//   j_set(p, j0)      0/1 class of the sub-tile starting at j0 (warp-uniform)
+//   set_boundary(p)   first j of the second class (kTwoSets only)
 //   load_j(p, j, w)   global -> registers, one j point per lane
-//   kTwoSets          j_set can return 1
+//   kTwoSets          the j range holds two classes (deformed / target)
 //   pair<SET>(I, w, acc)        accumulate one pair interaction
 //   finalize(p, row, acc)       consume the full FP64 row sums; returns a value
 //                               that is summed over the tile
@@ -38,16 +39,16 @@ namespace lddmm {
 
 namespace cg = cooperative_groups;
 
-// One staged 32-point sub-tile against the warp's two rows.  SET is the
-// compile-time class of the sub-tile (the varifold's deformed / target halves), so
-// the accumulator index is static and the arrays stay in registers.
+// Entries [lo, hi) of one staged 32-point sub-tile against the warp's two rows.  SET
+// is the compile-time class of those entries (the varifold's deformed / target
+// halves), so the accumulator index is static and the arrays stay in registers.
 template <int SET, class Op>
-__device__ __forceinline__ void run_sub(const Op &op, const float4 (*sj)[kSub],
+__device__ __forceinline__ void run_sub(const Op &op, const float4 (*sj)[kSub], int lo, int hi,
                                         const typename Op::IData &I0,
                                         const typename Op::IData &I1, float (&a0)[Op::NA],
                                         float (&a1)[Op::NA]) {
 #pragma unroll 8
-  for (int jj = 0; jj < kSub; ++jj) {
+  for (int jj = lo; jj < hi; ++jj) {
     float4 w[Op::JW];
 #pragma unroll
     for (int x = 0; x < Op::JW; ++x) w[x] = sj[x][jj];
@@ -68,7 +69,9 @@ __global__ void __launch_bounds__(W * 32) sweep_kernel(const Op op, const int2 *
 
   const int item = blockIdx.x / S;
   const int rank = blockIdx.x - item * S;
-  const int2 it = items[item];
+  const int2 it = items[item];  // static work list
+  pdl_wait();
+  pdl_trigger();
   const int p = it.x, tile = it.y;
   if (!op.active(p)) return;  // identical for every CTA of the cluster
 
@@ -81,32 +84,36 @@ __global__ void __launch_bounds__(W * 32) sweep_kernel(const Op op, const int2 *
 #pragma unroll
   for (int a = 0; a < NA; ++a) hi0[a] = lo0[a] = hi1[a] = lo1[a] = 0.0f;
 
-  const int nsub = op.j_count(p) / kSub;
-  const int step = S * W;
-  int k = rank * W + warp;
+  // every warp of the cluster takes one contiguous, equal (+-1) share of the j range
+  const int J = op.j_count(p);
+  const int nw = S * W, gw = rank * W + warp;
+  const int jb = (int)((long long)J * gw / nw), je = (int)((long long)J * (gw + 1) / nw);
+  const int split = Op::kTwoSets ? op.set_boundary(p) : J;
   float4 nxt[JW];
-  if (k < nsub) op.load_j(p, k * kSub + lane, nxt);
-  while (k < nsub) {
+  if (jb + lane < je) op.load_j(p, jb + lane, nxt);
+  for (int j0 = jb; j0 < je; j0 += kSub) {
     __syncwarp();
 #pragma unroll
     for (int x = 0; x < JW; ++x) s_j[warp][x][lane] = nxt[x];
     __syncwarp();
-    const int kn = k + step;
-    const int set = op.j_set(p, k * kSub);
-    if (kn < nsub) op.load_j(p, kn * kSub + lane, nxt);
+    const int cnt = min(kSub, je - j0);
+    const int jn = j0 + kSub;
+    if (jn + lane < je) op.load_j(p, jn + lane, nxt);
     float a0[NA], a1[NA];
 #pragma unroll
     for (int a = 0; a < NA; ++a) a0[a] = a1[a] = 0.0f;
-    if (Op::kTwoSets && set)
-      run_sub<1>(op, s_j[warp], I0, I1, a0, a1);
-    else
-      run_sub<0>(op, s_j[warp], I0, I1, a0, a1);
+    if (Op::kTwoSets) {
+      const int b = min(max(split - j0, 0), cnt);  // [0, b) first set, [b, cnt) second
+      if (b > 0) run_sub<0>(op, s_j[warp], 0, b, I0, I1, a0, a1);
+      if (b < cnt) run_sub<1>(op, s_j[warp], b, cnt, I0, I1, a0, a1);
+    } else {
+      run_sub<0>(op, s_j[warp], 0, cnt, I0, I1, a0, a1);
+    }
 #pragma unroll
     for (int a = 0; a < NA; ++a) {
       two_sum_acc(hi0[a], lo0[a], a0[a]);
       two_sum_acc(hi1[a], lo1[a], a1[a]);
     }
-    k = kn;
   }
 
 #pragma unroll

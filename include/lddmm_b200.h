@@ -221,6 +221,12 @@ int lddmm_ctx_time_sweeps(lddmm_ctx *ctx, int reps, double *ms4);
  * summed over pairs.  Returns the number of values written (at most n). */
 int lddmm_ctx_counters(const lddmm_ctx *ctx, long long *out, int n);
 
+/* Device-side timeline of the last L-BFGS cycle (or objective evaluation), from
+ * %globaltimer stamps the cooperative kernels write: us6 = entry and exit, in
+ * microseconds relative to the forward sweep's entry, of the forward time-loop sweep,
+ * the backward time-loop sweep and the fused optimiser update (-1 when not run). */
+int lddmm_ctx_timeline(const lddmm_ctx *ctx, double *us6);
+
 /* FP32 FMA throughput of this GPU (TFLOP/s, FMA = 2 flops) measured by a probe
  * kernel of independent FMA chains over every SM; the roofline denominator of the
  * FP32-bound sweeps.  Returns 0 and writes the figure to *tflops. */

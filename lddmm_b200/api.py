@@ -90,6 +90,13 @@ class Context:
         check(lib.lddmm_ctx_time_sweeps(self._h, reps, dptr(ms)))
         return dict(shoot=ms[0], adjoint=ms[1], varifold=ms[2], eval=ms[3])
 
+    def timeline(self):
+        """Last cycle's device timeline (microseconds from the forward sweep's entry):
+        entry/exit of the forward sweep, backward sweep and optimiser update."""
+        t = np.zeros(6)
+        check(lib.lddmm_ctx_timeline(self._h, dptr(t)))
+        return dict(fwd=(t[0], t[1]), bwd=(t[2], t[3]), opt=(t[4], t[5]))
+
     def counters(self):
         o = (C.c_longlong * 4)()
         check(lib.lddmm_ctx_counters(self._h, o, 4))

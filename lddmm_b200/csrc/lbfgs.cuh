@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "layout.h"
+#include "persist.cuh"
 
 namespace lddmm {
 
@@ -65,13 +66,11 @@ __device__ __forceinline__ void store_trial_f32(const VecArgs &A, const PairDesc
   f[((size_t)t * A.NPtot + P.pt_off + i) * 4 + d] = (float)x;
 }
 
-// One vector pass.  `k` = two-loop pass index for kTwoLoopB / kTwoLoopF.
-__global__ void __launch_bounds__(kVecThreads) vec_pass_kernel(VecArgs A, int mode, int k) {
+// One vector pass over chunk c.  `k` = two-loop pass index for kTwoLoopB / kTwoLoopF.
+// Called by a whole CTA (it synchronises the CTA).
+__device__ void vec_pass_chunk(const VecArgs &A, int mode, int k, int c) {
   __shared__ double s_scal[4];
   __shared__ double s_scr[kVecThreads / 32];
-  pdl_wait();
-  pdl_trigger();
-  const int c = blockIdx.x;
   const int p = A.chunk_pair[c];
   const PairDesc &P = A.pd[p];
   PairState &S = A.st[p];
@@ -239,6 +238,14 @@ __global__ void __launch_bounds__(kVecThreads) vec_pass_kernel(VecArgs A, int mo
     A.part_out[(size_t)c * 3 + 1] = d1;
     A.part_out[(size_t)c * 3 + 2] = d2;
   }
+  __syncthreads();
+}
+
+// One vector pass as its own launch (one CTA per chunk).
+__global__ void __launch_bounds__(kVecThreads) vec_pass_kernel(VecArgs A, int mode, int k) {
+  pdl_wait();
+  pdl_trigger();
+  vec_pass_chunk(A, mode, k, blockIdx.x);
 }
 
 __device__ __forceinline__ double serial_partial(const double *part, int c0, int nc, int j) {
@@ -248,12 +255,8 @@ __device__ __forceinline__ double serial_partial(const double *part, int c0, int
 }
 
 // After POST.  One thread per pair.  Records (f, |g|, step, evals) per iteration.
-__global__ void decide_kernel(const PairDesc *__restrict__ pd, PairState *st, int P,
-                              const double *__restrict__ part, OptParams o, double *rec) {
-  pdl_wait();
-  pdl_trigger();
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P) return;
+__device__ void decide_pair(const PairDesc *__restrict__ pd, PairState *st, int p,
+                            const double *__restrict__ part, const OptParams &o, double *rec) {
   PairState &S = st[p];
   const PairDesc &D = pd[p];
   S.action = kActNone;
@@ -341,14 +344,18 @@ __global__ void decide_kernel(const PairDesc *__restrict__ pd, PairState *st, in
   S.hisNum = (S.itr <= o.mem_num) ? S.itr - 1 : o.mem_num;
 }
 
-// After FIN.  Starts the line search of pairs with a new direction
-// (lineSearch.cpp:34-55) and sets the evaluation flags for the next sweep.
-__global__ void ls_init_kernel(const PairDesc *__restrict__ pd, PairState *st, int P,
-                               const double *__restrict__ part, int *act) {
+__global__ void decide_kernel(const PairDesc *__restrict__ pd, PairState *st, int P,
+                              const double *__restrict__ part, OptParams o, double *rec) {
   pdl_wait();
   pdl_trigger();
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P) return;
+  if (p < P) decide_pair(pd, st, p, part, o, rec);
+}
+
+// After FIN.  Starts the line search of pairs with a new direction
+// (lineSearch.cpp:34-55) and sets the evaluation flags for the next sweep.
+__device__ void ls_init_pair(const PairDesc *__restrict__ pd, PairState *st, int p,
+                             const double *__restrict__ part, int *act) {
   PairState &S = st[p];
   const PairDesc &D = pd[p];
   if (S.need_dir) {
@@ -372,6 +379,90 @@ __global__ void ls_init_kernel(const PairDesc *__restrict__ pd, PairState *st, i
   }
   S.active = (S.phase == kPhaseInit || S.phase == kPhaseLS) ? 1 : 0;
   act[p] = S.active;
+}
+
+__global__ void ls_init_kernel(const PairDesc *__restrict__ pd, PairState *st, int P,
+                               const double *__restrict__ part, int *act) {
+  pdl_wait();
+  pdl_trigger();
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < P) ls_init_pair(pd, st, p, part, act);
+}
+
+// The whole optimiser update of one cycle in one cooperative launch: the passes of
+// the per-kernel sequence (POST, DECIDE, ACCEPT, B_0..B_{m-1}, F_0..F_{m-1}, FIN,
+// LSINIT) run as grid-stride loops over the chunks, separated by grid barriers
+// (bounded waits, persist.cuh).  Same arithmetic and reduction order as the per-kernel
+// sequence.  part[0] / part[1] alternate exactly as there.
+// Loop control of a device-side L-BFGS loop (CUDA graph WHILE node): counts the cycle
+// and keeps the loop running while some pair is active and the cycle bound is not
+// reached.  Called by one CTA after the pairs' states are final for this cycle.
+__device__ void cycle_control(cudaGraphConditionalHandle h, const int *act, int P, int *cyc,
+                              int max_cycles) {
+  __shared__ int s_any;
+  if (threadIdx.x == 0) s_any = 0;
+  __syncthreads();
+  int any = 0;
+  for (int p = threadIdx.x; p < P; p += blockDim.x) any |= act[p];
+  if (any) atomicOr(&s_any, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int n = ++(*cyc);
+    cudaGraphSetConditional(h, (s_any && n < max_cycles) ? 1u : 0u);
+  }
+}
+
+__global__ void cycle_control_kernel(cudaGraphConditionalHandle h, const int *act, int P,
+                                     int *cyc, int max_cycles) {
+  pdl_wait();
+  cycle_control(h, act, P, cyc, max_cycles);
+}
+
+__global__ void __launch_bounds__(kVecThreads)
+    lbfgs_cycle_kernel(VecArgs A, OptParams o, double *part0, double *part1, double *rec,
+                       int *act, int P, int nchunk, StepSync *sy, cudaGraphConditionalHandle h,
+                       int *cyc, int max_cycles) {
+  pdl_wait();
+  stamp_entry(sy, 2);
+  unsigned int phase = 0;
+  auto barrier = [&]() -> bool {
+    ++phase;
+    return grid_barrier(sy, phase * gridDim.x, 1000u + phase);
+  };
+  int s = 0;  // pass sequence number: writes part[s & 1], reads part[(s + 1) & 1]
+  auto pass = [&](int mode, int k) {
+    A.part_out = (s & 1) ? part1 : part0;
+    A.part_in = (s & 1) ? part0 : part1;
+    for (int c = blockIdx.x; c < nchunk; c += gridDim.x) vec_pass_chunk(A, mode, k, c);
+    ++s;
+  };
+  pass(kPost, 0);
+  if (!barrier()) return;
+  if (blockIdx.x == 0)
+    for (int p = threadIdx.x; p < P; p += blockDim.x) decide_pair(A.pd, A.st, p, part0, o, rec);
+  if (!barrier()) return;
+  pass(kAccept, 0);
+  if (!barrier()) return;
+  for (int k = 0; k < o.mem_num; ++k) {
+    pass(kTwoLoopB, k);
+    if (!barrier()) return;
+  }
+  for (int k = 0; k < o.mem_num; ++k) {
+    pass(kTwoLoopF, k);
+    if (!barrier()) return;
+  }
+  pass(kFin, 0);
+  if (!barrier()) return;
+  if (blockIdx.x == 0) {
+    const double *last = ((s - 1) & 1) ? part1 : part0;
+    for (int p = threadIdx.x; p < P; p += blockDim.x) ls_init_pair(A.pd, A.st, p, last, act);
+    if (cyc) {
+      __syncthreads();
+      cycle_control(h, act, P, cyc, max_cycles);
+    }
+  }
+  stamp_exit(sy, 2);
+  pdl_trigger();
 }
 
 }  // namespace lddmm

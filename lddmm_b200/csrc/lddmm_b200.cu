@@ -82,7 +82,8 @@ struct lddmm_ctx {
   // persistent multi-step sweeps (one cooperative launch per direction)
   bool persistent = false;
   int pers_grid[2] = {0, 0};  // CTAs of the forward / backward persistent kernel
-  int n_units = 0;            // (pair, 8-row group) work units
+  int n_units = 0;            // (pair, row group) work units
+  int cycle_grid = 0;         // CTAs of the fused L-BFGS cycle kernel (0: per-pass launches)
   int2 *units = nullptr;
   StepSync *sync = nullptr;
 
@@ -110,7 +111,13 @@ struct lddmm_ctx {
 
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // device-side L-BFGS loop: a graph whose WHILE node repeats the cycle
+  cudaGraphExec_t loop_exec = nullptr;
+  bool loop_valid = false;
+  OptParams loop_opt{};
+  int *cyc = nullptr;  // cycles run by the device loop
   long long last_cycles = 0, last_launches = 0, last_evals = 0;
+  int lbfgs_calls = 0;  // graphs are captured from the second L-BFGS call on
   bool use_graph = true;
   cudaGraphExec_t cycle_exec = nullptr;
   OptParams graph_opt{};
@@ -136,6 +143,8 @@ static void dfree(T *&p) {
 
 lddmm_ctx::~lddmm_ctx() {
   if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
+  if (loop_exec) cudaGraphExecDestroy(loop_exec);
+  dfree(cyc);
   dfree(pd); dfree(act); dfree(st); dfree(qs); dfree(as); dfree(us); dfree(ls);
   dfree(q64); dfree(p64); dfree(ec); dfree(en); dfree(el); dfree(tc); dfree(tn); dfree(tl);
   dfree(e64);
@@ -330,13 +339,19 @@ static bool pick_def(int order, lddmm_ctx &c) {
   return false;
 }
 
+template <int D, char CT, char DT>
+static void set_vfd(lddmm_ctx &c) {
+  c.varifold = varifold_impl<D, CT, DT>;
+  c.tt = tt_impl<D, CT, DT>;
+}
+
 template <int D, char CT>
 static bool pick_vfd_dt(char dt, lddmm_ctx &c) {
   switch (dt) {
-    case 'B': c.varifold = varifold_impl<D, CT, 'B'>; c.tt = tt_impl<D, CT, 'B'>; return true;
-    case 'L': c.varifold = varifold_impl<D, CT, 'L'>; c.tt = tt_impl<D, CT, 'L'>; return true;
-    case 'O': c.varifold = varifold_impl<D, CT, 'O'>; c.tt = tt_impl<D, CT, 'O'>; return true;
-    case 'U': c.varifold = varifold_impl<D, CT, 'U'>; c.tt = tt_impl<D, CT, 'U'>; return true;
+    case 'B': set_vfd<D, CT, 'B'>(c); return true;
+    case 'L': set_vfd<D, CT, 'L'>(c); return true;
+    case 'O': set_vfd<D, CT, 'O'>(c); return true;
+    case 'U': set_vfd<D, CT, 'U'>(c); return true;
   }
   return false;
 }
@@ -808,6 +823,11 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
       c.pers_grid[0] = std::min(b0 * sms, c.n_units);
       c.pers_grid[1] = std::min(b1 * sms, c.n_units);
     }
+    int bc = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bc, lbfgs_cycle_kernel, kVecThreads, 0) ==
+            cudaSuccess &&
+        bc > 0 && cf.persistent >= 0)
+      c.cycle_grid = std::min(bc * sms, c.nchunk_tot);
   }
   if (cf.autotune) {
     const int rc = autotune(c);
@@ -1006,7 +1026,10 @@ static cudaError_t ensure_lbfgs_buffers(lddmm_ctx &c, int m, int rec_cap) {
   return cudaSuccess;
 }
 
-static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o) {
+// One cycle: objective sweep of the trial points, then the optimiser update.  With a
+// conditional handle the cycle also drives the device-side loop (cycle_control).
+static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o,
+                                cudaGraphConditionalHandle h = 0, int max_cycles = 0) {
   CUE(run_eval(c, c.GT, nullptr, nullptr, true));
   VecArgs A;
   A.pd = c.pd;
@@ -1021,6 +1044,22 @@ static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o) {
   A.m = o.mem_num;
   const unsigned nb = (unsigned)c.nchunk_tot;
   const int pb = (c.P + 127) / 128;
+  if (c.cycle_grid > 0) {
+    // the whole optimiser update in one cooperative launch
+    CUE(cudaMemsetAsync(&c.sync->arrive, 0, sizeof(unsigned int), c.stream));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)c.cycle_grid);
+    cfg.blockDim = dim3(kVecThreads);
+    cfg.stream = c.stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, lbfgs_cycle_kernel, A, o, c.part[0], c.part[1], c.rec, c.act,
+                              c.P, c.nchunk_tot, c.sync, h, max_cycles > 0 ? c.cyc : nullptr,
+                              max_cycles);
+  }
   int s = 0;  // pass sequence number: writes part[s & 1], reads part[(s - 1) & 1]
   auto pass = [&](int mode, int k) -> cudaError_t {
     A.part_out = c.part[s & 1];
@@ -1036,14 +1075,21 @@ static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o) {
   for (int k = 0; k < o.mem_num; ++k) CUE(pass(kTwoLoopB, k));
   for (int k = 0; k < o.mem_num; ++k) CUE(pass(kTwoLoopF, k));
   CUE(pass(kFin, 0));
-  return launch(ls_init_kernel, (unsigned)pb, 128, 0, c.stream, (const PairDesc *)c.pd, c.st, c.P,
-                (const double *)c.part[(s - 1) & 1], c.act);
+  CUE(launch(ls_init_kernel, (unsigned)pb, 128, 0, c.stream, (const PairDesc *)c.pd, c.st, c.P,
+             (const double *)c.part[(s - 1) & 1], c.act));
+  if (max_cycles > 0)
+    CUE(launch(cycle_control_kernel, 1, 256, 0, c.stream, h, (const int *)c.act, c.P, c.cyc,
+               max_cycles));
+  return cudaSuccess;
 }
 
 static long long kernels_per_cycle(const lddmm_ctx &c, int m) {
-  // objective: T shooting + [geometry + varifold] + gather + objective + T adjoint;
-  // optimiser: POST, DECIDE, ACCEPT, m + m two-loop passes, FIN, LSINIT
-  return 2LL * c.T + 2 + (c.has_vfd ? 2 : 0) + 2LL * m + 5;
+  // objective: T shooting + [geometry + varifold] + gather + objective + T adjoint
+  // (2 launches when the time loops are persistent); optimiser: POST, DECIDE, ACCEPT,
+  // m + m two-loop passes, FIN, LSINIT (1 launch when fused)
+  const long long sweeps = c.persistent ? 2 : 2LL * c.T;
+  const long long opt = c.cycle_grid > 0 ? 1 : 2LL * m + 5;
+  return sweeps + 2 + (c.has_vfd ? 2 : 0) + opt;
 }
 
 static bool same_opt(const OptParams &a, const OptParams &b) {
@@ -1070,6 +1116,53 @@ static int build_graph(lddmm_ctx &c, const OptParams &o) {
   c.graph_opt = o;
   c.graph_valid = true;
   return 0;
+}
+
+// The whole L-BFGS loop as one graph: a WHILE conditional node whose body is one
+// cycle; the cycle's last kernel sets the condition (some pair active and fewer than
+// max_cycles cycles run).  Returns false (and leaves no partial state) when the
+// runtime cannot build it; the caller then drives the cycles from the host.
+static bool build_loop_graph(lddmm_ctx &c, const OptParams &o, int max_cycles) {
+  if (c.loop_valid && same_opt(c.loop_opt, o)) return true;
+  if (c.loop_exec) {
+    cudaGraphExecDestroy(c.loop_exec);
+    c.loop_exec = nullptr;
+  }
+  c.loop_valid = false;
+  if (!c.cyc && dalloc(&c.cyc, 1) != cudaSuccess) return false;
+  cudaGraph_t g = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
+  bool ok = false;
+  cudaGraphConditionalHandle h = 0;
+  cudaGraphNode_t node;
+  cudaGraphNodeParams np = {};
+  if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess) {
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    if (cudaGraphAddNode(&node, g, nullptr, 0, &np) == cudaSuccess) {
+      cudaGraph_t body = np.conditional.phGraph_out[0];
+      if (cudaStreamBeginCaptureToGraph(c.stream, body, nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const cudaError_t e = launch_cycle(c, o, h, max_cycles);
+        cudaGraph_t captured = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(c.stream, &captured);
+        ok = (e == cudaSuccess && e2 == cudaSuccess);
+      }
+    }
+  }
+  if (ok) ok = cudaGraphInstantiate(&c.loop_exec, g, 0) == cudaSuccess;
+  cudaGraphDestroy(g);
+  cudaGetLastError();  // clear a refused capture or instantiation
+  if (!ok) {
+    if (c.loop_exec) cudaGraphExecDestroy(c.loop_exec);
+    c.loop_exec = nullptr;
+    return false;
+  }
+  c.loop_opt = o;
+  c.loop_valid = true;
+  return true;
 }
 
 static void print_table(const lddmm_ctx &c, int p, const std::vector<double> &rec, int rows) {
@@ -1118,20 +1211,40 @@ static int lbfgs_run(lddmm_ctx &c, const lddmm_opt *opt, const double *alp, bool
   CU(launch_set_active(c, c.P));
   CU(load_trial(c, alp, host));
   CU(cudaMemcpyAsync(c.X, c.XT, sizeof(double) * c.nvar, cudaMemcpyDeviceToDevice, c.stream));
-  if (c.use_graph) {
-    const int rc = build_graph(c, o);
-    if (rc) return rc;
-  }
   // safety bound on cycles: every iteration takes at most bisMax + epdMax + 2
   // evaluations (>= 62); the per-pair state machine ends well before this.
   const long long max_cycles = (long long)o.itr_max * 200 + 8;
   std::vector<int> hact(c.P);
   long long cycles = 0;
-  const int check_every = 4;
+  const int check_every = 8;
   bool timed_out = false;
-  while (true) {
+  // Capturing and instantiating the loop graph costs far more than one registration's
+  // launches, so a context's first L-BFGS call drives the cycles from the host with
+  // direct launches; later calls run the whole loop as one device-side graph.
+  const bool graphs = c.use_graph && c.lbfgs_calls++ > 0;
+  if (graphs && max_cycles < (1LL << 30) && build_loop_graph(c, o, (int)max_cycles)) {
+    // the whole loop on the device: one launch, one synchronisation
+    CU(cudaMemsetAsync(c.cyc, 0, sizeof(int), c.stream));
+    CU(cudaGraphLaunch(c.loop_exec, c.stream));
+    int ncyc = 0;
+    CU(cudaMemcpyAsync(hact.data(), c.act, sizeof(int) * c.P, cudaMemcpyDeviceToHost, c.stream));
+    CU(cudaMemcpyAsync(&ncyc, c.cyc, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    CU(cudaStreamSynchronize(c.stream));
+    {
+      const int rc = check_sync(c);
+      if (rc) return rc;
+    }
+    cycles = ncyc;
+    for (int a : hact) timed_out |= (a != 0);
+  }
+  const bool host_loop = !graphs || !c.loop_valid;
+  if (host_loop && graphs) {
+    const int rc = build_graph(c, o);
+    if (rc) return rc;
+  }
+  while (host_loop) {
     for (int k = 0; k < check_every; ++k) {
-      if (c.use_graph)
+      if (graphs)
         CU(cudaGraphLaunch(c.cycle_exec, c.stream));
       else
         CU(launch_cycle(c, o));
@@ -1211,6 +1324,21 @@ extern "C" int lddmm_lbfgs_trace(const lddmm_ctx *ctx, int pair, double *rows4, 
                  cudaMemcpyDeviceToHost) != cudaSuccess)
     return LDDMM_ERR_CUDA;
   return n;
+}
+
+extern "C" int lddmm_ctx_timeline(const lddmm_ctx *ctx, double *us6) {
+  if (!ctx || !us6 || !ctx->sync) return LDDMM_ERR_ARG;
+  StepSync h;
+  if (cudaMemcpy(&h, ctx->sync, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    set_err("lddmm_ctx_timeline: %s", cudaGetErrorString(cudaGetLastError()));
+    return LDDMM_ERR_CUDA;
+  }
+  const double t0 = (double)h.stamp[0][0];
+  for (int k = 0; k < 3; ++k) {
+    us6[2 * k] = h.stamp[k][0] ? ((double)h.stamp[k][0] - t0) * 1e-3 : -1.0;
+    us6[2 * k + 1] = h.stamp[k][1] ? ((double)h.stamp[k][1] - t0) * 1e-3 : -1.0;
+  }
+  return 0;
 }
 
 extern "C" int lddmm_ctx_counters(const lddmm_ctx *ctx, long long *out, int n) {

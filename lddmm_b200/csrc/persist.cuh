@@ -38,7 +38,25 @@ constexpr int kPersistWarps = 8;          // warps per persistent CTA
 struct StepSync {
   unsigned int arrive;  // grid barrier arrivals, reset to 0 before every launch
   unsigned int error;   // nonzero: a barrier wait timed out (1 + step index)
+  // timeline of the cooperative kernels of the last cycle (%globaltimer, ns):
+  // [slot][0] entry of CTA 0, [slot][1] latest CTA exit; slots: 0 forward sweep,
+  // 1 backward sweep, 2 optimiser update
+  unsigned long long stamp[4][2];
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void stamp_entry(StepSync *sy, int slot) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) sy->stamp[slot][0] = global_ns();
+}
+
+__device__ __forceinline__ void stamp_exit(StepSync *sy, int slot) {
+  if (threadIdx.x == 0) atomicMax(&sy->stamp[slot][1], global_ns());
+}
 
 constexpr unsigned int kSpinLimit = 1u << 22;  // polls: a few seconds at most
 
@@ -91,6 +109,7 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 2)
   __shared__ PairDesc s_pd;  // descriptor of the unit in hand, kept across steps
   __shared__ int s_unit[3];  // unit index, pair, active flag
   pdl_wait();
+  stamp_entry(sy, dir > 0 ? 0 : 1);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int lrow = lane % kRowPairs, lg = lane / kRowPairs;
   if (threadIdx.x == 0) s_unit[0] = -1;
@@ -205,6 +224,7 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 2)
     }
     if (!grid_barrier(sy, (unsigned)(s + 1) * gridDim.x, (unsigned)s)) return;
   }
+  stamp_exit(sy, dir > 0 ? 0 : 1);
   pdl_trigger();
 }
 

@@ -396,9 +396,10 @@ __global__ void ls_init_kernel(const PairDesc *__restrict__ pd, PairState *st, i
 // sequence.  part[0] / part[1] alternate exactly as there.
 // Loop control of a device-side L-BFGS loop (CUDA graph WHILE node): counts the cycle
 // and keeps the loop running while some pair is active and the cycle bound is not
-// reached.  Called by one CTA after the pairs' states are final for this cycle.
+// reached and no persistent sweep's barrier has timed out (error word).  Called by one
+// CTA after the pairs' states are final for this cycle.
 __device__ void cycle_control(cudaGraphConditionalHandle h, const int *act, int P, int *cyc,
-                              int max_cycles) {
+                              int max_cycles, const StepSync *sy) {
   __shared__ int s_any;
   if (threadIdx.x == 0) s_any = 0;
   __syncthreads();
@@ -408,14 +409,15 @@ __device__ void cycle_control(cudaGraphConditionalHandle h, const int *act, int 
   __syncthreads();
   if (threadIdx.x == 0) {
     const int n = ++(*cyc);
-    cudaGraphSetConditional(h, (s_any && n < max_cycles) ? 1u : 0u);
+    const bool err = *(volatile const unsigned int *)&sy->error != 0u;
+    cudaGraphSetConditional(h, (s_any && n < max_cycles && !err) ? 1u : 0u);
   }
 }
 
 __global__ void cycle_control_kernel(cudaGraphConditionalHandle h, const int *act, int P,
-                                     int *cyc, int max_cycles) {
+                                     int *cyc, int max_cycles, const StepSync *sy) {
   pdl_wait();
-  cycle_control(h, act, P, cyc, max_cycles);
+  cycle_control(h, act, P, cyc, max_cycles, sy);
 }
 
 __global__ void __launch_bounds__(kVecThreads)
@@ -436,29 +438,39 @@ __global__ void __launch_bounds__(kVecThreads)
     for (int c = blockIdx.x; c < nchunk; c += gridDim.x) vec_pass_chunk(A, mode, k, c);
     ++s;
   };
-  pass(kPost, 0);
-  if (!barrier()) return;
-  if (blockIdx.x == 0)
-    for (int p = threadIdx.x; p < P; p += blockDim.x) decide_pair(A.pd, A.st, p, part0, o, rec);
-  if (!barrier()) return;
-  pass(kAccept, 0);
-  if (!barrier()) return;
-  for (int k = 0; k < o.mem_num; ++k) {
-    pass(kTwoLoopB, k);
-    if (!barrier()) return;
-  }
-  for (int k = 0; k < o.mem_num; ++k) {
-    pass(kTwoLoopF, k);
-    if (!barrier()) return;
-  }
-  pass(kFin, 0);
-  if (!barrier()) return;
-  if (blockIdx.x == 0) {
-    const double *last = ((s - 1) & 1) ? part1 : part0;
-    for (int p = threadIdx.x; p < P; p += blockDim.x) ls_init_pair(A.pd, A.st, p, last, act);
-    if (cyc) {
-      __syncthreads();
-      cycle_control(h, act, P, cyc, max_cycles);
+  bool ok = true;
+  do {  // one pass; a timed-out barrier breaks out to the loop-control exit below
+    pass(kPost, 0);
+    if (!(ok = barrier())) break;
+    if (blockIdx.x == 0)
+      for (int p = threadIdx.x; p < P; p += blockDim.x) decide_pair(A.pd, A.st, p, part0, o, rec);
+    if (!(ok = barrier())) break;
+    pass(kAccept, 0);
+    if (!(ok = barrier())) break;
+    for (int k = 0; k < o.mem_num && ok; ++k) {
+      pass(kTwoLoopB, k);
+      ok = barrier();
+    }
+    for (int k = 0; k < o.mem_num && ok; ++k) {
+      pass(kTwoLoopF, k);
+      ok = barrier();
+    }
+    if (!ok) break;
+    pass(kFin, 0);
+    if (!(ok = barrier())) break;
+    if (blockIdx.x == 0) {
+      const double *last = ((s - 1) & 1) ? part1 : part0;
+      for (int p = threadIdx.x; p < P; p += blockDim.x) ls_init_pair(A.pd, A.st, p, last, act);
+    }
+  } while (false);
+  if (blockIdx.x == 0 && cyc) {
+    // drives the device-side loop; after a timed-out barrier (error word set) the loop
+    // must end, whatever the pairs' state
+    __syncthreads();
+    if (ok) {
+      cycle_control(h, act, P, cyc, max_cycles, sy);
+    } else if (threadIdx.x == 0) {
+      cudaGraphSetConditional(h, 0u);
     }
   }
   stamp_exit(sy, 2);

@@ -1079,7 +1079,7 @@ static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o,
              (const double *)c.part[(s - 1) & 1], c.act));
   if (max_cycles > 0)
     CUE(launch(cycle_control_kernel, 1, 256, 0, c.stream, h, (const int *)c.act, c.P, c.cyc,
-               max_cycles));
+               max_cycles, (const StepSync *)c.sync));
   return cudaSuccess;
 }
 
@@ -1199,6 +1199,7 @@ static int lbfgs_run(lddmm_ctx &c, const lddmm_opt *opt, const double *alp, bool
   o.rec_cap = std::min(opt->itr_max + 1, 100001);
   CU(cudaSetDevice(c.device));
   CU(ensure_lbfgs_buffers(c, o.mem_num, o.rec_cap));
+  CU(reset_sync(c));
   // initial state: every pair evaluates its starting point
   std::vector<PairState> hs(c.P);
   for (auto &s : hs) {

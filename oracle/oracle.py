@@ -235,3 +235,50 @@ class Reference:
         self.lib.ref_dq_kernel(_d(dq), _d(q), _d(l), _d(r), C.c_int(order), C.c_double(width),
                                C.c_int(q.shape[0]), C.c_int(q.shape[1]))
         return dq
+
+
+class ReferenceCuda:
+    """The reference's plain FP64 GPU path (CUDA/src, cuBLAS) compiled in place
+    (oracle/_ref/librefcu{2,3}d.so, ``make -C oracle refcu``) behind a project host
+    driver that replaces its MEX entry (CUDA/src/LDDMM.cu:13-151).  Same argument
+    meaning and C++ layouts as :class:`Reference`.  Needs a GPU; measurement and test
+    infrastructure only."""
+
+    def __init__(self, dim: int):
+        path = os.path.join(HERE, "_ref", f"librefcu{dim}d.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} missing: run `make -C oracle refcu`")
+        self.dim = dim
+        self.lib = C.CDLL(path)
+        assert self.lib.refcu_dim() == dim
+
+    @staticmethod
+    def available(dim: int = 3) -> bool:
+        return os.path.exists(os.path.join(HERE, "_ref", f"librefcu{dim}d.so"))
+
+    _common = Reference._common
+
+    def objgrd(self, P, alp):
+        assert P.dim == self.dim
+        alp = np.ascontiguousarray(alp, dtype=np.float64).reshape(-1)
+        g = np.zeros_like(alp)
+        f = C.c_double()
+        rc = self.lib.refcu_objgrd(*self._common(P), _d(alp), C.byref(f), _d(g))
+        if rc:
+            raise RuntimeError(f"refcu_objgrd rc={rc}")
+        return f.value, g
+
+    def lbfgs(self, P, alp0, itr_max=300, tol=1e-6, wolfe1=1e-4, wolfe2=0.9, mem_num=5,
+              verbose=False):
+        """One registration; returns status, momenta, final objective, evaluations and
+        the milliseconds spent inside LBFGS (CUDA events) and in the whole call."""
+        assert P.dim == self.dim
+        x = np.ascontiguousarray(alp0, dtype=np.float64).reshape(-1).copy()
+        out = np.zeros(4)
+        ret = self.lib.refcu_lbfgs(*self._common(P), C.c_int(itr_max), C.c_double(tol),
+                                   C.c_double(wolfe1), C.c_double(wolfe2), C.c_int(mem_num),
+                                   C.c_int(1 if verbose else 0), _d(x), _d(out))
+        if ret < 0:
+            raise RuntimeError(f"refcu_lbfgs rc={ret}")
+        return dict(ret=ret, x=x, f=float(out[3]), evals=int(out[2]), ms_lbfgs=float(out[0]),
+                    ms_total=float(out[1]))

@@ -463,6 +463,7 @@ __global__ void __launch_bounds__(kVecThreads)
       for (int p = threadIdx.x; p < P; p += blockDim.x) ls_init_pair(A.pd, A.st, p, last, act);
     }
   } while (false);
+  if (ok) grid_depart(sy);
   if (blockIdx.x == 0 && cyc) {
     // drives the device-side loop; after a timed-out barrier (error word set) the loop
     // must end, whatever the pairs' state

@@ -51,6 +51,8 @@ void set_err(const char *fmt, ...) {
   } while (0)
 
 constexpr int kWarps = 4;  // warps per sweep CTA
+// persistent sweeps are chosen automatically up to this many row groups per resident CTA
+constexpr int kPersistAutoUnits = 2;
 
 template <class T>
 cudaError_t dalloc(T **p, size_t n) {
@@ -81,10 +83,16 @@ struct lddmm_ctx {
   int S_shoot = 1, S_adj = 1, S_vfd = 1;
   // persistent multi-step sweeps (one cooperative launch per direction)
   bool persistent = false;
-  int pers_grid[2] = {0, 0};  // CTAs of the forward / backward persistent kernel
+  int pers_ctas = 0;          // CTAs of the persistent kernels (one share of work each)
   int n_units = 0;            // (pair, row group) work units
+  int n_segs = 0, n_slots = 0;
   int cycle_grid = 0;         // CTAs of the fused L-BFGS cycle kernel (0: per-pass launches)
   int2 *units = nullptr;
+  int4 *segs = nullptr;       // persistent work plan (persist.cuh)
+  int *cta_seg = nullptr;
+  int2 *unit_parts = nullptr;
+  double *seg_part = nullptr;
+  unsigned int *unit_cnt = nullptr;
   StepSync *sync = nullptr;
 
   // device memory
@@ -152,7 +160,8 @@ lddmm_ctx::~lddmm_ctx() {
   dfree(reg_part); dfree(vfd_part); dfree(f_dev); dfree(pt_items); dfree(el_items);
   dfree(chunk_pair); dfree(X); dfree(G); dfree(XT); dfree(GT); dfree(Dv); dfree(Qv);
   dfree(Sh); dfree(Yh); dfree(part[0]); dfree(part[1]); dfree(rec); dfree(sync);
-  dfree(units);
+  dfree(units); dfree(segs); dfree(cta_seg); dfree(unit_parts); dfree(seg_part);
+  dfree(unit_cnt);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -230,12 +239,18 @@ static cudaError_t adjoint_impl(lddmm_ctx &c, int t, double *g, double *pdot) {
 }
 
 // Cooperative launch of a persistent multi-step sweep (all CTAs co-resident; the
-// runtime refuses the launch otherwise).  The barrier counter is reset first.
+// runtime refuses the launch otherwise).
 template <class Op>
-static cudaError_t launch_persistent(lddmm_ctx &c, const Op &op, int dir, int grid) {
-  CUE(cudaMemsetAsync(&c.sync->arrive, 0, sizeof(unsigned int), c.stream));
+static cudaError_t launch_persistent(lddmm_ctx &c, const Op &op, int dir) {
+  SweepPlan plan;
+  plan.units = c.units;
+  plan.segs = c.segs;
+  plan.cta_seg = c.cta_seg;
+  plan.unit_parts = c.unit_parts;
+  plan.part = c.seg_part;
+  plan.cnt = c.unit_cnt;
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)grid);
+  cfg.gridDim = dim3((unsigned)c.pers_ctas);
   cfg.blockDim = dim3(kPersistWarps * 32);
   cfg.stream = c.stream;
   cudaLaunchAttribute attr[1];
@@ -243,8 +258,7 @@ static cudaError_t launch_persistent(lddmm_ctx &c, const Op &op, int dir, int gr
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, persistent_sweep_kernel<Op>, op, (const int2 *)c.units,
-                            c.n_units, c.T, dir, c.sync);
+  return cudaLaunchKernelEx(&cfg, persistent_sweep_kernel<Op>, op, plan, c.T, dir, c.sync);
 }
 
 template <int D, int ORDER>
@@ -260,7 +274,7 @@ static cudaError_t shoot_all_impl(lddmm_ctx &c, double *vlc) {
   op.reg0 = c.reg_part;
   op.NP = c.NPtot;
   op.ntile = c.ngrp_tot;
-  return launch_persistent(c, op, +1, c.pers_grid[0]);
+  return launch_persistent(c, op, +1);
 }
 
 template <int D, int ORDER>
@@ -277,7 +291,7 @@ static cudaError_t adjoint_all_impl(lddmm_ctx &c, double *g) {
   op.us0 = c.us;
   op.ls0 = c.ls;
   op.NP = c.NPtot;
-  return launch_persistent(c, op, -1, c.pers_grid[1]);
+  return launch_persistent(c, op, -1);
 }
 
 template <int D, int ORDER>
@@ -493,6 +507,70 @@ extern "C" int lddmm_elm_ifo(const int *elm_vtx, int vpe, int elm_num, int nde_n
       }
     }
   return rows;
+}
+
+// Work plan of the persistent sweeps: the step's work (row groups x their j ranges,
+// laid end to end in unit order) cut into G contiguous shares, one per CTA.  Cuts
+// inside a row group are rounded to the 32-entry sub-tile and moved to the row group's
+// edge when they would leave a part shorter than kMinPart entries.  With little work
+// per CTA (under kSplitMin entries) row groups are not cut at all: each CTA takes whole
+// row groups and G is at most the row-group count.
+struct HostPlan {
+  std::vector<int4> segs;       // (unit, j begin, j end, part) in CTA order
+  std::vector<int> cta_seg;     // G + 1 offsets into segs
+  std::vector<int2> unit_parts; // (parts, first partial slot)
+  int slots = 0;
+};
+
+constexpr long long kMinPart = 128;
+constexpr long long kSplitMin = 512;
+
+static HostPlan plan_sweeps(const std::vector<int2> &units, const std::vector<PairDesc> &hpd,
+                            int G_max) {
+  const int nu = (int)units.size();
+  std::vector<long long> us(nu + 1, 0);
+  for (int u = 0; u < nu; ++u) us[u + 1] = us[u] + hpd[units[u].x].Npad;
+  const long long W = us[nu];
+  const bool cut = W / std::max(G_max, 1) >= kSplitMin;
+  const int G = cut ? G_max : std::max(1, std::min(G_max, nu));
+  std::vector<long long> b(G + 1, 0);
+  b[G] = W;
+  for (int k = 1; k < G; ++k) {
+    long long x;
+    if (cut) {
+      const long long w = W * k / G;
+      int u = (int)(std::upper_bound(us.begin(), us.end(), w) - us.begin()) - 1;
+      u = std::min(std::max(u, 0), nu - 1);
+      const long long J = us[u + 1] - us[u];
+      long long off = (w - us[u] + kSub / 2) / kSub * kSub;
+      if (off < kMinPart) off = 0;
+      else if (J - off < kMinPart) off = J;
+      x = us[u] + off;
+    } else {
+      x = us[(long long)nu * k / G];
+    }
+    b[k] = std::max(b[k - 1], std::min(x, W));
+  }
+  HostPlan h;
+  h.cta_seg.assign(G + 1, 0);
+  h.unit_parts.assign(nu, make_int2(0, 0));
+  std::vector<int> parts(nu, 0);
+  int u0 = 0;
+  for (int k = 0; k < G; ++k) {
+    h.cta_seg[k] = (int)h.segs.size();
+    while (u0 < nu && us[u0 + 1] <= b[k]) ++u0;
+    for (int v = u0; v < nu && us[v] < b[k + 1]; ++v) {
+      const long long lo = std::max(b[k], us[v]) - us[v];
+      const long long hi = std::min(b[k + 1], us[v + 1]) - us[v];
+      if (hi > lo) h.segs.push_back(make_int4(v, (int)lo, (int)hi, parts[v]++));
+    }
+  }
+  h.cta_seg[G] = (int)h.segs.size();
+  for (int v = 0; v < nu; ++v) {
+    h.unit_parts[v] = make_int2(parts[v], h.slots);
+    if (parts[v] > 1) h.slots += parts[v];
+  }
+  return h;
 }
 
 static int default_cluster(int n_items) {
@@ -813,15 +891,27 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
     CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
     const int b0 = c.pers_blocks(0), b1 = c.pers_blocks(1);
     const int cap = std::min(b0, b1) * sms;
-    // automatic: when every row group gets its own resident CTA (one wave) a step is
-    // latency-bound and the persistent sweep wins; bigger batches keep per-step
-    // launches, whose two-rows-per-lane 64-row tiles are cheaper per pair
+    // automatic: up to a few row groups per resident CTA the persistent sweep wins (a
+    // step is a few microseconds and the plan balances any row-group count); bigger
+    // batches keep per-step launches, whose 64-row tiles are cheaper per pair
     c.persistent = cap > 0 && (cf.persistent > 0 ||
-                               (cf.persistent == 0 && c.n_units <= cap));
+                               (cf.persistent == 0 && c.n_units <= kPersistAutoUnits * cap));
     CU(dalloc(&c.sync, 1));
     if (c.persistent) {
-      c.pers_grid[0] = std::min(b0 * sms, c.n_units);
-      c.pers_grid[1] = std::min(b1 * sms, c.n_units);
+      const HostPlan h = plan_sweeps(uni, c.hpd, cap);
+      c.pers_ctas = (int)h.cta_seg.size() - 1;
+      c.n_segs = (int)h.segs.size();
+      c.n_slots = h.slots;
+      CU(dalloc(&c.segs, c.n_segs));
+      CU(dalloc(&c.cta_seg, h.cta_seg.size()));
+      CU(dalloc(&c.unit_parts, h.unit_parts.size()));
+      CU(dalloc(&c.seg_part, (size_t)std::max(c.n_slots, 1) * kGroup * kPartNA));
+      CU(dalloc(&c.unit_cnt, std::max(c.n_units, 1)));
+      CU(cudaMemcpy(c.segs, h.segs.data(), sizeof(int4) * h.segs.size(), cudaMemcpyHostToDevice));
+      CU(cudaMemcpy(c.cta_seg, h.cta_seg.data(), sizeof(int) * h.cta_seg.size(),
+                    cudaMemcpyHostToDevice));
+      CU(cudaMemcpy(c.unit_parts, h.unit_parts.data(), sizeof(int2) * h.unit_parts.size(),
+                    cudaMemcpyHostToDevice));
     }
     int bc = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bc, lbfgs_cycle_kernel, kVecThreads, 0) ==
@@ -837,9 +927,14 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   return 0;
 }
 
-// Clears the persistent sweeps' barrier and error words (start of every entry point).
+// Clears the persistent kernels' barrier / error words and the split row groups'
+// arrival counts (start of every entry point; after a clean launch they are zero
+// already, after a timed-out one they are not).
 static cudaError_t reset_sync(lddmm_ctx &c) {
-  return cudaMemsetAsync(c.sync, 0, 2 * sizeof(unsigned int), c.stream);
+  CUE(cudaMemsetAsync(c.sync, 0, 4 * sizeof(unsigned int), c.stream));
+  if (c.unit_cnt)
+    CUE(cudaMemsetAsync(c.unit_cnt, 0, sizeof(unsigned int) * c.n_units, c.stream));
+  return cudaSuccess;
 }
 
 // LDDMM_ERR_TIMEOUT when a persistent sweep's grid barrier gave up (stream must be
@@ -1046,7 +1141,6 @@ static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o,
   const int pb = (c.P + 127) / 128;
   if (c.cycle_grid > 0) {
     // the whole optimiser update in one cooperative launch
-    CUE(cudaMemsetAsync(&c.sync->arrive, 0, sizeof(unsigned int), c.stream));
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)c.cycle_grid);
     cfg.blockDim = dim3(kVecThreads);

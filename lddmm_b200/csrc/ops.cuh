@@ -81,22 +81,41 @@ struct ShootOp {
     acc[1] = fmaf(K, w[1].y, acc[1]);
     if (D == 3) acc[D - 1] = fmaf(K, w[1].z, acc[D - 1]);
   }
-  __device__ double finalize(int p, int row, const double (&v)[NA]) const {
+  // finalize operands (loaded before the row sums are complete): q_t and a_t of the row
+  struct FData {
+    double q[3], a[3];
+  };
+  __device__ void fin_load(int p, int row, FData &F) const {
+    const PairDesc &P = pd[p];
+    if (row >= P.N) return;
+    const size_t g = (size_t)P.pt_off + row;
+    const double *a = x64 + P.var_off + ((size_t)t * P.N + row) * D;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      F.q[d] = __ldcg(&q64_t[g * D + d]);
+      F.a[d] = __ldcg(&a[d]);
+    }
+  }
+  __device__ double finalize(int p, int row, const double (&v)[NA], const FData &F) const {
     const PairDesc &P = pd[p];
     if (row >= P.N) return 0.0;
     const size_t g = (size_t)P.pt_off + row;
-    const double *a = x64 + P.var_off + ((size_t)t * P.N + row) * D;
     double e = 0.0, qn[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-      qn[d] = q64_t[g * D + d] + P.dt * v[d];
+      qn[d] = F.q[d] + P.dt * v[d];
       q64_n[g * D + d] = qn[d];
-      e += a[d] * v[d];
+      e += F.a[d] * v[d];
       if (vlc64) vlc64[g * D + d] = v[d];
     }
     const double s = P.kscale;
     qs_n[g] = make_float4((float)(qn[0] * s), (float)(qn[1] * s), (float)(qn[2] * s), 0.0f);
     return e;
+  }
+  __device__ double finalize(int p, int row, const double (&v)[NA]) const {
+    FData F;
+    fin_load(p, row, F);
+    return finalize(p, row, v, F);
   }
   __device__ void write_tile(int p, int tile, double v) const {
     tile_part[pd[p].itile_off + tile] = v;
@@ -212,7 +231,18 @@ struct AdjointOp {
       acc[D + d] = fmaf(s, dq[d], acc[D + d]);
     }
   }
-  __device__ double finalize(int p, int row, const double (&v)[NA]) const {
+  // finalize operand loaded before the row sums are complete: p of the row
+  struct FData {
+    double p[3];
+  };
+  __device__ void fin_load(int p, int row, FData &F) const {
+    const PairDesc &P = pd[p];
+    if (row >= P.N) return;
+    const size_t g = (size_t)P.pt_off + row;
+#pragma unroll
+    for (int d = 0; d < D; ++d) F.p[d] = __ldcg(&p64[g * D + d]);
+  }
+  __device__ double finalize(int p, int row, const double (&v)[NA], const FData &F) const {
     const PairDesc &P = pd[p];
     if (row >= P.N) return 0.0;
     const size_t g = (size_t)P.pt_off + row;
@@ -222,7 +252,7 @@ struct AdjointOp {
       const double pdot = P.pd_fac * v[D + d];
       if (pdot64) pdot64[g * D + d] = pdot;
       if (g64) g64[P.var_off + ((size_t)t * P.N + row) * D + d] = P.dt * v[d];
-      pn[d] = p64[g * D + d] - P.dt * pdot;
+      pn[d] = F.p[d] - P.dt * pdot;
       p64[g * D + d] = pn[d];
     }
     if (t > 0 && us_n) {
@@ -237,6 +267,11 @@ struct AdjointOp {
       ls_n[g] = make_float4((float)l[0], (float)l[1], (float)l[2], 0.0f);
     }
     return 0.0;
+  }
+  __device__ double finalize(int p, int row, const double (&v)[NA]) const {
+    FData F;
+    fin_load(p, row, F);
+    return finalize(p, row, v, F);
   }
   __device__ void write_tile(int, int, double) const {}
   __device__ void write_group(int, int, double) const {}

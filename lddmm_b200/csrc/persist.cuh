@@ -4,24 +4,36 @@
 // The steps are sequential (step t + 1 reads the positions / adjoint state step t
 // finalised) and, for one registration of a few thousand landmarks, one step is only
 // a few microseconds of arithmetic.  Per-step launches then spend most of their time
-// ramping CTAs up and down and in the cross-CTA reduction of split j ranges.  Here:
+// ramping CTAs up and down.  Here:
 //
 //   * every CTA stays resident for the whole recursion; steps are separated by a
 //     grid barrier;
-//   * a work unit is a row group of kGroup = 16 rows of one pair, and its CTA covers
-//     the whole j range: the 8 warps take equal contiguous shares, and inside a warp
-//     lane l handles rows l % 8 and l % 8 + 8 against every 4th point of each staged
+//   * the work of a step is the list of row groups (kGroup = 16 rows of one pair)
+//     times their j ranges, laid end to end and cut into one contiguous share per CTA
+//     (host-side plan, snapped to 32-entry boundaries): every CTA gets the same number
+//     of pair interactions whatever the row-group count, so no SM idles at the barrier
+//     while another runs a second row group.  A CTA's share is a list of segments
+//     (row group, j range), taken two at a time ("rounds");
+//   * in a round the 8 warps are dealt to the (one or two) segments in proportion to
+//     their lengths and take equal contiguous shares of their segment's j range; lane
+//     l handles rows l % 8 and l % 8 + 8 against every 4th point of each staged
 //     32-point sub-tile (lane group l / 8), so each staged operand serves two pairs;
-//   * reductions stay inside the CTA: a shuffle butterfly over the 4 lane groups, then
-//     the 8 warps through shared memory in warp order, all in FP64 after the per-tile
-//     TwoSum, so results are bit-reproducible;
-//   * the unit's first 8 threads finalise its rows (Euler step / adjoint update).
+//   * reductions: a shuffle butterfly over the 4 lane groups, then the segment's warps
+//     through shared memory in warp order, in FP64 after the per-tile TwoSum.  A row
+//     group cut over several CTAs stores one FP64 partial per part; the CTA that
+//     completes the row group's arrival count (whichever it is) adds the parts in part
+//     order and finalises, so results are bit-reproducible for a given plan;
+//   * each segment of a round has its own 16-thread epilogue group (lanes 0-15 of warp
+//     0 or of warp 1): both run at once, with warp-level synchronisation only.
 //
-// The grid barrier is a monotonically increasing arrival counter (reset before the
-// launch).  Every wait is bounded: after kSpinLimit polls the CTA records the step in
-// the error word and leaves the kernel, so a launch that is not fully co-resident ends
-// with an error instead of hanging.  The launch uses the cooperative attribute, with
-// which the runtime refuses a grid that cannot be co-resident.
+// Grid barrier: a monotonically increasing arrival count (fire-and-forget atomic
+// add) that the CTAs poll against (step + 1) x grid.  When a launch ends, each CTA
+// counts its departure after its last wait; the last one to leave zeroes both counts,
+// so the next launch starts from zero without a memset.  Every wait is bounded: after
+// kSpinLimit polls the CTA records the step in the error word and leaves the kernel,
+// so a launch that is not fully co-resident ends with an error instead of hanging (the
+// host then clears the words).  The launch uses the cooperative attribute, with which
+// the runtime refuses a grid that cannot be co-resident.
 #pragma once
 
 #include "common.cuh"
@@ -36,8 +48,10 @@ constexpr int kLaneGroups = 32 / kRowPairs;  // j interleave inside a warp
 constexpr int kPersistWarps = 8;          // warps per persistent CTA
 
 struct StepSync {
-  unsigned int arrive;  // grid barrier arrivals, reset to 0 before every launch
+  unsigned int arrive;  // grid barrier arrivals since the launch began
   unsigned int error;   // nonzero: a barrier wait timed out (1 + step index)
+  unsigned int depart;  // CTAs past their last wait (resets arrive at launch end)
+  unsigned int pad_;
   // timeline of the cooperative kernels of the last cycle (%globaltimer, ns):
   // [slot][0] entry of CTA 0, [slot][1] latest CTA exit; slots: 0 forward sweep,
   // 1 backward sweep, 2 optimiser update
@@ -58,7 +72,7 @@ __device__ __forceinline__ void stamp_exit(StepSync *sy, int slot) {
   if (threadIdx.x == 0) atomicMax(&sy->stamp[slot][1], global_ns());
 }
 
-constexpr unsigned int kSpinLimit = 1u << 22;  // polls: a few seconds at most
+constexpr unsigned int kSpinLimit = 1u << 23;  // polls: a few seconds at most
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
   unsigned int v;
@@ -66,23 +80,35 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
   return v;
 }
 
-// Returns false when the wait timed out (the caller must leave the kernel).
+__device__ __forceinline__ unsigned int ld_relaxed(const unsigned int *p) {
+  unsigned int v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Waits until `target` arrivals (this CTA's included) have been counted.  Returns
+// false when the wait timed out (the caller must leave the kernel without departing).
+// `tag` identifies the wait in the error word.  The poll is one relaxed load per
+// iteration (the error word is read every 64th); the fence after the loop orders the
+// CTA's later reads after the arrivals it observed.
 __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
-                                             unsigned int step) {
+                                             unsigned int tag) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
+    int ok = 1;
     __threadfence();
     atomicAdd(&sy->arrive, 1u);
-    int ok = 1;
     unsigned int n = 0;
-    while (ld_acquire(&sy->arrive) < target) {
-      if (ld_acquire(&sy->error) != 0u || ++n > kSpinLimit) {
-        atomicCAS(&sy->error, 0u, 1u + step);
-        ok = 0;
-        break;
+    while (ld_relaxed(&sy->arrive) < target) {
+      if ((++n & 63u) == 0u) {
+        if (ld_relaxed(&sy->error) != 0u || n > kSpinLimit) {
+          atomicCAS(&sy->error, 0u, 1u + tag);
+          ok = 0;
+          break;
+        }
+        if (n > 4096u) __nanosleep(64);
       }
-      __nanosleep(32);
     }
     __threadfence();
     s_ok = ok;
@@ -91,139 +117,217 @@ __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
   return s_ok != 0;
 }
 
+// After a CTA's last grid_barrier: the last CTA to depart zeroes the counts.  Every
+// CTA has stopped polling `arrive` by then.
+__device__ __forceinline__ void grid_depart(StepSync *sy) {
+  if (threadIdx.x == 0) {
+    const unsigned int old = atomicAdd(&sy->depart, 1u);
+    if (old == gridDim.x - 1) {
+      sy->arrive = 0u;
+      sy->depart = 0u;
+    }
+  }
+}
+
+// Work plan of the persistent sweeps (built on the host when the context is created).
+struct SweepPlan {
+  const int2 *units;      // (pair, row group) per unit
+  const int4 *segs;       // (unit, j begin, j end, part) in CTA order
+  const int *cta_seg;     // CTA k owns segs[cta_seg[k] .. cta_seg[k + 1])
+  const int2 *unit_parts; // (parts, first partial slot) per unit
+  double *part;           // FP64 partials [slot][kGroup][kPartNA]
+  unsigned int *cnt;      // per-unit arrival count of split row groups (self-resetting)
+};
+
+constexpr int kPartNA = 6;  // accumulators per row in a partial slot (>= every Op::NA)
+
 // Op: the sweep interface of sweep.cuh plus set_step(t) (pointers of time step t) and
-// write_group(p, k, v) (row-group partial of a kTileSum op).  units: (pair, row group).
+// write_group(p, k, v) (row-group partial of a kTileSum op).
 // dir = +1 runs t = 0..T-1, dir = -1 runs t = T-1..0.
-// Two CTAs per SM (<= 128 registers): a single registration of a few thousand
-// landmarks then has all its row groups resident at once.
+// Two CTAs per SM (<= 128 registers), 16 warps per SM.
 template <class Op>
 __global__ void __launch_bounds__(kPersistWarps * 32, 2)
-    persistent_sweep_kernel(Op op, const int2 *__restrict__ units, int n_units, int T, int dir,
-                            StepSync *sy) {
+    persistent_sweep_kernel(Op op, SweepPlan plan, int T, int dir, StepSync *sy) {
   constexpr int JW = Op::JW;
   constexpr int NA = Op::NA;
   constexpr int NW = kPersistWarps;
+  static_assert(NA <= kPartNA, "partial slot too small");
   __shared__ float4 s_j[NW][JW][kSub];
   __shared__ double s_red[NW][kGroup][NA];
-  __shared__ double s_scr[NW];
-  __shared__ PairDesc s_pd;  // descriptor of the unit in hand, kept across steps
-  __shared__ int s_unit[3];  // unit index, pair, active flag
+  __shared__ PairDesc s_pd[2];  // descriptors of the round's units
+  __shared__ int s_uinf[2][2];  // per round slot: pair | group << 16, active
   pdl_wait();
   stamp_entry(sy, dir > 0 ? 0 : 1);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int lrow = lane % kRowPairs, lg = lane / kRowPairs;
-  if (threadIdx.x == 0) s_unit[0] = -1;
+  const int s0 = plan.cta_seg[blockIdx.x], s1 = plan.cta_seg[blockIdx.x + 1];
+  const bool one_round = s1 - s0 <= 2;  // descriptors loaded once for the whole launch
   for (int s = 0; s < T; ++s) {
     const int t = dir > 0 ? s : T - 1 - s;
     Op o = op;
     o.set_step(t);
-    for (int u = blockIdx.x; u < n_units; u += gridDim.x) {
-      __syncthreads();
-      if (s_unit[0] != u) {  // uniform; a CTA with one unit loads it once
-        __syncthreads();
-        if (threadIdx.x == 0) {
-          const int2 un = units[u];
-          s_unit[0] = u;
-          s_unit[1] = un.x | (un.y << 16);
-          s_unit[2] = op.active(un.x);
-          s_pd = op.pd[un.x];
+    for (int k = s0; k < s1; k += 2) {
+      const int nseg = min(2, s1 - k);
+      const int4 sa = plan.segs[k];
+      const int4 sb = nseg > 1 ? plan.segs[k + 1] : make_int4(0, 0, 0, 0);
+      if (!one_round || s == 0) {
+        __syncthreads();  // the previous round's epilogue is done with s_pd / s_uinf
+        if (threadIdx.x < nseg) {
+          const int2 un = plan.units[threadIdx.x == 0 ? sa.x : sb.x];
+          s_uinf[threadIdx.x][0] = un.x | (un.y << 16);
+          s_uinf[threadIdx.x][1] = op.active(un.x);
+          s_pd[threadIdx.x] = op.pd[un.x];
         }
         __syncthreads();
       }
-      if (!s_unit[2]) continue;  // uniform for the CTA
-      const int grp = s_unit[1] >> 16;
-      o.pd = &s_pd;  // the op reads descriptor 0 from shared memory from here on
-      const int p = 0;
-      typename Op::IData I0, I1;
-      o.load_i(p, grp * kGroup + lrow, I0);
-      o.load_i(p, grp * kGroup + kRowPairs + lrow, I1);
-      float hi0[NA], lo0[NA], hi1[NA], lo1[NA];
+      // warps dealt to the segments in proportion to their lengths (>= 1 each)
+      const int la = sa.z - sa.y, lb = nseg > 1 ? sb.z - sb.y : 0;
+      const int wa = nseg > 1 ? min(NW - 1, max(1, (int)((2LL * NW * la + la + lb) /
+                                                           (2LL * (la + lb)))))
+                              : NW;
+      const int g = warp < wa ? 0 : 1;  // this warp's segment (warp-uniform)
+      if (s_uinf[g][1]) {
+        const int4 sg = g ? sb : sa;
+        const int wl = g ? warp - wa : warp, nw = g ? NW - wa : wa;
+        const int grp = s_uinf[g][0] >> 16;
+        o.pd = &s_pd[g];  // the op reads descriptor 0 from shared memory from here on
+        const int p = 0;
+        typename Op::IData I0, I1;
+        o.load_i(p, grp * kGroup + lrow, I0);
+        o.load_i(p, grp * kGroup + kRowPairs + lrow, I1);
+        float hi0[NA], lo0[NA], hi1[NA], lo1[NA];
 #pragma unroll
-      for (int a = 0; a < NA; ++a) hi0[a] = lo0[a] = hi1[a] = lo1[a] = 0.0f;
-      const int J = o.j_count(p);
-      const int jb = (int)((long long)J * warp / NW), je = (int)((long long)J * (warp + 1) / NW);
-      const int split = Op::kTwoSets ? o.set_boundary(p) : J;
-      float4 nxt[JW];
-      float acc0[NA], acc1[NA];
-      if (jb + lane < je) o.load_j(p, jb + lane, nxt);
-      for (int j0 = jb; j0 < je; j0 += kSub) {
-        __syncwarp();
+        for (int a = 0; a < NA; ++a) hi0[a] = lo0[a] = hi1[a] = lo1[a] = 0.0f;
+        const int L = sg.z - sg.y;
+        const int jb = sg.y + (int)((long long)L * wl / nw);
+        const int je = sg.y + (int)((long long)L * (wl + 1) / nw);
+        const int split = Op::kTwoSets ? o.set_boundary(p) : sg.z;
+        float4 nxt[JW];
+        float acc0[NA], acc1[NA];
+        if (jb + lane < je) o.load_j(p, jb + lane, nxt);
+        for (int j0 = jb; j0 < je; j0 += kSub) {
+          __syncwarp();
 #pragma unroll
-        for (int x = 0; x < JW; ++x) s_j[warp][x][lane] = nxt[x];
-        __syncwarp();
-        const int cnt = min(kSub, je - j0);
-        const int jn = j0 + kSub;
-        if (jn + lane < je) o.load_j(p, jn + lane, nxt);
-        const bool fresh = ((j0 - jb) & (4 * kSub - 1)) == 0;
-        if (fresh) {
+          for (int x = 0; x < JW; ++x) s_j[warp][x][lane] = nxt[x];
+          __syncwarp();
+          const int cnt = min(kSub, je - j0);
+          const int jn = j0 + kSub;
+          if (jn + lane < je) o.load_j(p, jn + lane, nxt);
+          const bool fresh = ((j0 - jb) & (4 * kSub - 1)) == 0;
+          if (fresh) {
 #pragma unroll
-          for (int a = 0; a < NA; ++a) acc0[a] = acc1[a] = 0.0f;
-        }
-        const int b = Op::kTwoSets ? min(max(split - j0, 0), cnt) : cnt;
+            for (int a = 0; a < NA; ++a) acc0[a] = acc1[a] = 0.0f;
+          }
+          const int b = Op::kTwoSets ? min(max(split - j0, 0), cnt) : cnt;
 #pragma unroll 4
-        for (int jj = lg; jj < b; jj += kLaneGroups) {
-          float4 w[JW];
-#pragma unroll
-          for (int x = 0; x < JW; ++x) w[x] = s_j[warp][x][jj];
-          o.template pair<0>(I0, w, acc0);
-          o.template pair<0>(I1, w, acc1);
-        }
-        if (Op::kTwoSets) {
-          // first entry >= b that belongs to this lane group
-          const int b1 = b + ((lg - b) % kLaneGroups + kLaneGroups) % kLaneGroups;
-#pragma unroll 4
-          for (int jj = b1; jj < cnt; jj += kLaneGroups) {
+          for (int jj = lg; jj < b; jj += kLaneGroups) {
             float4 w[JW];
 #pragma unroll
             for (int x = 0; x < JW; ++x) w[x] = s_j[warp][x][jj];
-            o.template pair<1>(I0, w, acc0);
-            o.template pair<1>(I1, w, acc1);
+            o.template pair<0>(I0, w, acc0);
+            o.template pair<0>(I1, w, acc1);
+          }
+          if (Op::kTwoSets) {
+            // first entry >= b that belongs to this lane group
+            const int b1 = b + ((lg - b) % kLaneGroups + kLaneGroups) % kLaneGroups;
+#pragma unroll 4
+            for (int jj = b1; jj < cnt; jj += kLaneGroups) {
+              float4 w[JW];
+#pragma unroll
+              for (int x = 0; x < JW; ++x) w[x] = s_j[warp][x][jj];
+              o.template pair<1>(I0, w, acc0);
+              o.template pair<1>(I1, w, acc1);
+            }
+          }
+          // fold into the compensated sum every 4 sub-tiles (<= 32 plain FP32 terms
+          // per lane) and after the last one
+          if (((j0 - jb) & (4 * kSub - 1)) == 3 * kSub || j0 + kSub >= je) {
+#pragma unroll
+            for (int a = 0; a < NA; ++a) {
+              two_sum_acc(hi0[a], lo0[a], acc0[a]);
+              two_sum_acc(hi1[a], lo1[a], acc1[a]);
+            }
           }
         }
-        // fold into the compensated sum every 4 sub-tiles (<= 32 plain FP32 terms per
-        // lane) and after the last one
-        if (((j0 - jb) & (4 * kSub - 1)) == 3 * kSub || j0 + kSub >= je) {
+        // lane groups -> lanes 0..7 (fixed butterfly)
 #pragma unroll
-          for (int a = 0; a < NA; ++a) {
-            two_sum_acc(hi0[a], lo0[a], acc0[a]);
-            two_sum_acc(hi1[a], lo1[a], acc1[a]);
+        for (int a = 0; a < NA; ++a) {
+          double v0 = (double)hi0[a] + (double)lo0[a];
+          double v1 = (double)hi1[a] + (double)lo1[a];
+#pragma unroll
+          for (int off = kRowPairs; off < 32; off <<= 1) {
+            v0 += __shfl_xor_sync(0xffffffffu, v0, off);
+            v1 += __shfl_xor_sync(0xffffffffu, v1, off);
           }
-        }
-      }
-      // lane groups -> lanes 0..7 (fixed butterfly), then warps in order
-#pragma unroll
-      for (int a = 0; a < NA; ++a) {
-        double v0 = (double)hi0[a] + (double)lo0[a];
-        double v1 = (double)hi1[a] + (double)lo1[a];
-#pragma unroll
-        for (int off = kRowPairs; off < 32; off <<= 1) {
-          v0 += __shfl_xor_sync(0xffffffffu, v0, off);
-          v1 += __shfl_xor_sync(0xffffffffu, v1, off);
-        }
-        if (lg == 0) {
-          s_red[warp][lrow][a] = v0;
-          s_red[warp][kRowPairs + lrow][a] = v1;
+          if (lg == 0) {
+            s_red[warp][lrow][a] = v0;
+            s_red[warp][kRowPairs + lrow][a] = v1;
+          }
         }
       }
       __syncthreads();
-      double e = 0.0;
-      if (threadIdx.x < kGroup) {
+      // epilogue: segment e on lanes 0-15 of warp e (both segments at once); the
+      // condition is uniform over those 16 lanes
+      const int e = warp;
+      if (e < nseg && lane < kGroup && s_uinf[e][1]) {
+        const int4 se = e ? sb : sa;
+        const int w0 = e ? wa : 0, w1 = e ? NW : wa;
+        const int grp_e = s_uinf[e][0] >> 16;
+        Op &oe = o;
+        oe.pd = &s_pd[e];
         double v[NA];
 #pragma unroll
         for (int a = 0; a < NA; ++a) {
           double x = 0.0;
-          for (int w = 0; w < NW; ++w) x += s_red[w][threadIdx.x][a];
+          for (int w = w0; w < w1; ++w) x += s_red[w][lane][a];
           v[a] = x;
         }
-        e = o.finalize(p, grp * kGroup + threadIdx.x, v);
-      }
-      if (Op::kTileSum) {
-        const double tot = block_sum(e, s_scr);
-        if (threadIdx.x == 0) o.write_group(p, grp, tot);
+        typename Op::FData F;  // finalize operands, in flight during the combine
+        oe.fin_load(0, grp_e * kGroup + lane, F);
+        const int2 up = plan.unit_parts[se.x];
+        bool fin = true;
+        if (up.x > 1) {
+          // row group cut over several CTAs: publish this part; the CTA completing the
+          // count adds all parts in part order
+          double *slot = plan.part + ((size_t)(up.y + se.w) * kGroup + lane) * kPartNA;
+#pragma unroll
+          for (int a = 0; a < NA; ++a) slot[a] = v[a];
+          __threadfence();
+          __syncwarp(0xffffu);
+          int last = 0;
+          if (lane == 0) {
+            last = atomicAdd(&plan.cnt[se.x], 1u) == (unsigned int)up.x - 1u;
+            if (last) {
+              plan.cnt[se.x] = 0u;  // next step's arrivals come after the grid barrier
+              __threadfence();
+            }
+          }
+          fin = __shfl_sync(0xffffu, last, 0) != 0;
+          __syncwarp(0xffffu);
+          if (fin) {
+#pragma unroll
+            for (int a = 0; a < NA; ++a) v[a] = 0.0;
+            for (int q = 0; q < up.x; ++q) {
+              const double *src = plan.part + ((size_t)(up.y + q) * kGroup + lane) * kPartNA;
+#pragma unroll
+              for (int a = 0; a < NA; ++a) v[a] += __ldcg(src + a);
+            }
+          }
+        }
+        if (fin) {
+          double en = oe.finalize(0, grp_e * kGroup + lane, v, F);
+          if (Op::kTileSum) {
+#pragma unroll
+            for (int off = kGroup / 2; off > 0; off >>= 1)
+              en += __shfl_xor_sync(0xffffu, en, off);
+            if (lane == 0) oe.write_group(0, grp_e, en);
+          }
+        }
       }
     }
     if (!grid_barrier(sy, (unsigned)(s + 1) * gridDim.x, (unsigned)s)) return;
   }
+  grid_depart(sy);
   stamp_exit(sy, dir > 0 ? 0 : 1);
   pdl_trigger();
 }

@@ -344,11 +344,11 @@ template <int D>
 static bool pick_def(int order, lddmm_ctx &c) {
   switch (order) {
     case -1: set_def<D, -1>(c); return true;
-    case 0: if (D == 3) { set_def<D, 0>(c); return true; } break;
-    case 1: if (D == 3) { set_def<D, 1>(c); return true; } break;
-    case 2: if (D == 3) { set_def<D, 2>(c); return true; } break;
-    case 3: if (D == 3) { set_def<D, 3>(c); return true; } break;
-    case 4: if (D == 3) { set_def<D, 4>(c); return true; } break;
+    case 0: set_def<D, 0>(c); return true;
+    case 1: set_def<D, 1>(c); return true;
+    case 2: set_def<D, 2>(c); return true;
+    case 3: set_def<D, 3>(c); return true;
+    case 4: set_def<D, 4>(c); return true;
   }
   return false;
 }
@@ -660,7 +660,7 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
     P.nchunk = (int)((P.var_num + kChunk - 1) / kChunk);
     P.dt = a.time_stp;
     P.dis_wgt = a.dis_wgt;
-    def_kernel_scales(a.knl_order, a.knl_width, &P.kscale, &P.pd_fac);
+    def_kernel_scales(a.knl_order, a.dim, a.knl_width, &P.kscale, &P.pd_fac);
     if (c.has_vfd) cen_kernel_scales(a.cen_knl_type, a.cen_knl_width, &P.cscale, &P.dc_fac);
     pt += P.Npad;
     el += P.Edpad;
@@ -1881,7 +1881,7 @@ extern "C" int lddmm_multiply_kernel_noalloc(int dim, int n, const double *d_q,
   desc.Npad = pad_to(n, kTile);
   desc.var_num = (long long)dim * n;
   desc.dt = 1.0;
-  def_kernel_scales(knl_order, knl_width, &desc.kscale, &desc.pd_fac);
+  def_kernel_scales(knl_order, dim, knl_width, &desc.kscale, &desc.pd_fac);
   const int ntiles = desc.Npad / kTile;
   noalloc_prepare_kernel<<<(desc.Npad + 255) / 256, 256, 0, st>>>(scratch, desc, d_q, d_a, n,
                                                                    desc.Npad, dim);

@@ -76,7 +76,7 @@ struct ShootOp {
       const float dz = I.z - w[0].z;
       nr2 = fmaf(-dz, dz, nr2);
     }
-    const float K = DefKernel<ORDER>::val(nr2);
+    const float K = DefKernelOf<D, ORDER>::type::val(nr2);
     acc[0] = fmaf(K, w[1].x, acc[0]);
     acc[1] = fmaf(K, w[1].y, acc[1]);
     if (D == 3) acc[D - 1] = fmaf(K, w[1].z, acc[D - 1]);
@@ -218,7 +218,7 @@ struct AdjointOp {
       nr2 = fmaf(-dq[d], dq[d], nr2);
     }
     float K, Wt;
-    DefKernel<ORDER>::val_w(nr2, K, Wt);
+    DefKernelOf<D, ORDER>::type::val_w(nr2, K, Wt);
     float lr = I.l[0] * rj[0];
 #pragma unroll
     for (int d = 1; d < D; ++d) lr = fmaf(I.l[d], rj[d], lr);

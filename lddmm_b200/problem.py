@@ -129,6 +129,20 @@ def circle_to_square(n_src: int = 200, n_tgt: int = 256, sigma_v: float = 0.5,
                    dir_width=0.0, dis_wgt=dis_wgt, name="circle2square")
 
 
+def circle_to_square_example(n_src: int = 500, n_tgt: int = 1000, half: float = 0.8) -> Problem:
+    """The reference's own 2D example (Cpp/examples/circle2square/run_circle2square.m:3-45),
+    restated: n_src points on the unit circle onto the boundary of [-half, half]^2
+    (n_tgt points, counter-clockwise from a corner), both closed polylines.  2D Matern
+    order 3 (Bessel K form) of width 0.025, varifold Cauchy(0.1) on segment centres x
+    Binet, weight 100, dt = 0.05 over 20 steps."""
+    src, se = shapes.circle(n_src)
+    tv, te = shapes.square_boundary(n_tgt, half)
+    cen, dr, vol = shapes.varifold_of(tv, te)
+    return Problem(src, se, cen, dr, vol, knl_order=3, knl_width=0.025, time_num=21,
+                   time_stp=0.05, cen_type="C", cen_width=0.1, dir_type="B", dir_width=0.0,
+                   dis_wgt=100.0, name="circle2square_example")
+
+
 def sphere_to_cube(subdiv: int = 4, cube_n: int = 32, knl_width: float = 0.4,
                    sigma_w: float = 0.15, time_num: int = 21, dis_wgt: float = 1.0,
                    knl_order: int = 1) -> Problem:

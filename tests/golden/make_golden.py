@@ -96,6 +96,20 @@ def circle2square():
          trace_f=r["trace_f"], trace_g2=r["trace_g2"], opt=np.array([40, 1e-6, 1e-4, 0.9, 5]))
 
 
+def circle2square_example():
+    """The reference's 2D example setting (2D Matern order 3, Cauchy centres)."""
+    P = problem.circle_to_square_example()
+    R = Reference(2)
+    rng = np.random.default_rng(11)
+    alp = rng.normal(size=P.var_num) * 0.02
+    f, g = R.objgrd(P, alp)
+    r = R.lbfgs(P, np.zeros(P.var_num), itr_max=15, tol=1e-2, wolfe1=0.0, wolfe2=0.5,
+                mem_num=10)
+    save("circle2square_example", P, alp=alp, f=np.array(f), g=g, x=r["x"],
+         f_lbfgs=np.array(r["f"]), ret=np.array(r["ret"]), trace_f=r["trace_f"],
+         trace_g2=r["trace_g2"], opt=np.array([15, 1e-2, 0.0, 0.5, 10]))
+
+
 def varifold_types():
     R = Reference(3)
     rng = np.random.default_rng(3)
@@ -161,6 +175,7 @@ if __name__ == "__main__":
     kernels(2, 1)
     kernels(3, 2)
     circle2square()
+    circle2square_example()
     sphere2cube_example()
     varifold_types()
     objgrd_orders_3d()

@@ -59,6 +59,21 @@ def test_lbfgs_trace_sphere2cube_example(api):
     early_trace_check(tr, zl["trace_f"], 8)
 
 
+def test_lbfgs_trace_circle2square_example(api):
+    """The reference's 2D example setting: 2D Matern order 3 (Bessel K form), Cauchy
+    centre kernel, Wolfe 0 / 0.5, memory 10.  The objective falls 200-fold within six
+    iterations here, so the FP32 path is pinned over the first five."""
+    z = golden("circle2square_example")
+    P = problem_from(z)
+    itr, tol, w1, w2, m = z["opt"]
+    with api.Context(P) as ctx:
+        x, res = ctx.lbfgs(np.zeros(P.var_num), itr_max=int(itr), tol=tol, wolfe1=w1,
+                           wolfe2=w2, mem_num=int(m))
+        tr = ctx.trace(0)
+    assert res[0]["status"] == int(z["ret"])
+    early_trace_check(tr, z["trace_f"], 5)
+
+
 def test_lbfgs_batch_equals_individual(api):
     """Each pair of a batch runs its own optimiser state: with the same launch shape
     (per-step sweeps, one CTA per tile) it follows exactly the path it takes alone."""

@@ -42,12 +42,19 @@ def test_dq_kernel_3d(api, order, tag):
         assert mrel(dq, ref) < TOL
 
 
-def test_kernels_2d_gaussian(api):
+@pytest.mark.parametrize("order,tag", ORDERS3)
+def test_kernels_2d(api, order, tag):
+    """2D: Gaussian and the Bessel-K Matern family (p0 = x^2 K0, p1 = x K1) of every
+    order; the order-0 dq sum is zero like the reference's."""
     z = golden("kernels_2d")
-    v = api.multiplyKernel(z["q"], z["a"], -1, float(z["width"]))
-    dq = api.dqKernel(z["q"], z["l"], z["a"], -1, float(z["width"]))
-    assert mrel(v, z["v_g"]) < TOL
-    assert mrel(dq, z["dq_g"]) < TOL
+    v = api.multiplyKernel(z["q"], z["a"], order, float(z["width"]))
+    dq = api.dqKernel(z["q"], z["l"], z["a"], order, float(z["width"]))
+    assert mrel(v, z[f"v_{tag}"]) < TOL
+    ref = z[f"dq_{tag}"]
+    if np.max(np.abs(ref)) == 0:
+        assert np.max(np.abs(dq)) == 0
+    else:
+        assert mrel(dq, ref) < TOL
 
 
 @pytest.mark.parametrize("dim", [2, 3])
@@ -73,6 +80,15 @@ def test_objgrd_circle2square_golden(api):
     assert rel(g, z["g"]) < TOL
 
 
+def test_objgrd_circle2square_example_golden(api):
+    """The reference's 2D example setting (2D Matern order 3, Cauchy centres)."""
+    z = golden("circle2square_example")
+    P = problem_from(z)
+    f, g = api.objgrd(P, z["alp"])
+    assert abs(f - float(z["f"])) / abs(float(z["f"])) < TOL
+    assert rel(g, z["g"]) < TOL
+
+
 def test_objgrd_sphere2cube_example_golden(api):
     """The reference's own example data (sphereData.mat / cubeData.mat, Cauchy centre
     kernel, Matern order 3, disWgt 100)."""
@@ -92,12 +108,13 @@ def test_objgrd_orders_3d_golden(api, order, tag):
     assert rel(g, z[f"g_{tag}"]) < TOL
 
 
-def test_objgrd_2d_gaussian_golden(api):
+@pytest.mark.parametrize("order,tag", ORDERS3)
+def test_objgrd_2d_golden(api, order, tag):
     z = golden("objgrd_orders_2d")
-    P = problem_from(z, knl_order=-1)
+    P = problem_from(z, knl_order=order)
     f, g = api.objgrd(P, z["alp"])
-    assert abs(f - float(z["f_g"])) / abs(float(z["f_g"])) < TOL
-    assert rel(g, z["g_g"]) < TOL
+    assert abs(f - float(z[f"f_{tag}"])) / abs(float(z[f"f_{tag}"])) < TOL
+    assert rel(g, z[f"g_{tag}"]) < TOL
 
 
 def test_objgrd_sphere2cube_full_size_vs_oracle(api, oracle):

@@ -30,6 +30,15 @@ def test_objgrd_circle2square(oracle):
     assert rel(g, z["g"]) < 1e-12
 
 
+def test_objgrd_circle2square_example(oracle):
+    """The reference's 2D example setting (2D Matern order 3 via p0 / p1, Cauchy)."""
+    z = golden("circle2square_example")
+    P = problem_from(z)
+    f, g = oracle.objgrd(P, z["alp"])
+    assert abs(f - float(z["f"])) / abs(float(z["f"])) < 1e-10
+    assert rel(g, z["g"]) < 1e-9
+
+
 def test_objgrd_sphere2cube_example(oracle):
     z = golden("sphere2cube_example")
     P = problem_from(z)

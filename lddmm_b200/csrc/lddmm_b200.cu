@@ -54,14 +54,66 @@ constexpr int kWarps = 4;  // warps per sweep CTA
 // persistent sweeps are chosen automatically up to this many row groups per resident CTA
 constexpr int kPersistAutoUnits = 2;
 
+// Device memory of the contexts comes from one stream-ordered pool per device, owned
+// by the library: allocation, zeroing and release are ordered on the context's stream,
+// and released blocks stay cached for the next context (up to kPoolKeepBytes), so
+// creating and destroying a context neither calls cudaMalloc / cudaFree nor waits for
+// the device.
+constexpr unsigned long long kPoolKeepBytes = 8ull << 30;
+constexpr int kMaxDevices = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[kMaxDevices] = {};
+
+cudaError_t device_pool(cudaMemPool_t *out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    e = cudaMemPoolCreate(&pool, &props);
+    if (e != cudaSuccess) return e;
+    unsigned long long keep = kPoolKeepBytes;
+    e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (e != cudaSuccess) {
+      cudaMemPoolDestroy(pool);
+      return e;
+    }
+    g_pool[dev] = pool;
+  }
+  *out = g_pool[dev];
+  return cudaSuccess;
+}
+
+// n zero-initialised elements, ordered on stream s (the current device's pool).
 template <class T>
-cudaError_t dalloc(T **p, size_t n) {
+cudaError_t dalloc(cudaStream_t s, T **p, size_t n) {
   *p = nullptr;
   if (n == 0) n = 1;
-  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
-  if (e == cudaSuccess) e = cudaMemset(*p, 0, n * sizeof(T));
+  cudaMemPool_t pool = nullptr;
+  cudaError_t e = device_pool(&pool);
+  if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)p, n * sizeof(T), pool, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(*p, 0, n * sizeof(T), s);
   return e;
 }
+
+// Scratch buffer released (stream-ordered) when it goes out of scope.
+template <class T>
+struct DevBuf {
+  T *p = nullptr;
+  cudaStream_t s = nullptr;
+  explicit DevBuf(cudaStream_t st) : s(st) {}
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, s);
+  }
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+};
 
 int pad_to(int n, int k) { return (n + k - 1) / k * k; }
 
@@ -144,24 +196,28 @@ struct lddmm_ctx {
 };
 
 template <class T>
-static void dfree(T *&p) {
-  if (p) cudaFree((void *)p);
+static void dfree(T *&p, cudaStream_t s) {
+  if (p) cudaFreeAsync((void *)p, s);
   p = nullptr;
 }
 
 lddmm_ctx::~lddmm_ctx() {
   if (cycle_exec) cudaGraphExecDestroy(cycle_exec);
   if (loop_exec) cudaGraphExecDestroy(loop_exec);
-  dfree(cyc);
-  dfree(pd); dfree(act); dfree(st); dfree(qs); dfree(as); dfree(us); dfree(ls);
-  dfree(q64); dfree(p64); dfree(ec); dfree(en); dfree(el); dfree(tc); dfree(tn); dfree(tl);
-  dfree(e64);
-  dfree(dcdd); dfree(tgt64); dfree(elm); dfree(pt_pair); dfree(adj_ptr); dfree(adj);
-  dfree(reg_part); dfree(vfd_part); dfree(f_dev); dfree(pt_items); dfree(el_items);
-  dfree(chunk_pair); dfree(X); dfree(G); dfree(XT); dfree(GT); dfree(Dv); dfree(Qv);
-  dfree(Sh); dfree(Yh); dfree(part[0]); dfree(part[1]); dfree(rec); dfree(sync);
-  dfree(units); dfree(segs); dfree(cta_seg); dfree(unit_parts); dfree(seg_part);
-  dfree(unit_cnt);
+  // stream-ordered releases: blocks return to the pool once the stream's work is done
+  dfree(cyc, stream); dfree(pd, stream); dfree(act, stream); dfree(st, stream);
+  dfree(qs, stream); dfree(as, stream); dfree(us, stream); dfree(ls, stream);
+  dfree(q64, stream); dfree(p64, stream); dfree(ec, stream); dfree(en, stream);
+  dfree(el, stream); dfree(tc, stream); dfree(tn, stream); dfree(tl, stream);
+  dfree(e64, stream); dfree(dcdd, stream); dfree(tgt64, stream); dfree(elm, stream);
+  dfree(pt_pair, stream); dfree(adj_ptr, stream); dfree(adj, stream); dfree(reg_part, stream);
+  dfree(vfd_part, stream); dfree(f_dev, stream); dfree(pt_items, stream);
+  dfree(el_items, stream); dfree(chunk_pair, stream); dfree(X, stream); dfree(G, stream);
+  dfree(XT, stream); dfree(GT, stream); dfree(Dv, stream); dfree(Qv, stream);
+  dfree(Sh, stream); dfree(Yh, stream); dfree(part[0], stream); dfree(part[1], stream);
+  dfree(rec, stream); dfree(sync, stream); dfree(units, stream); dfree(segs, stream);
+  dfree(cta_seg, stream); dfree(unit_parts, stream); dfree(seg_part, stream);
+  dfree(unit_cnt, stream);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -795,65 +851,79 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
       for (int i = 0; i < P.N; ++i) h_adjptr[P.pt_off + i + 1] = (int)h_adj.size();
   }
 
-  // ---- device memory
-  CU(dalloc(&c.pd, num));
-  CU(dalloc(&c.act, num));
-  CU(dalloc(&c.st, num));
-  CU(dalloc(&c.qs, (size_t)(c.T + 1) * c.NPtot));
-  CU(dalloc(&c.as, (size_t)c.T * c.NPtot));
-  CU(dalloc(&c.us, (size_t)2 * c.NPtot));
-  CU(dalloc(&c.ls, (size_t)2 * c.NPtot));
-  CU(dalloc(&c.q64, (size_t)(c.T + 1) * c.NPtot * D));
-  CU(dalloc(&c.p64, (size_t)c.NPtot * D));
-  CU(dalloc(&c.ec, std::max(c.EDtot, 1)));
-  CU(dalloc(&c.en, std::max(c.EDtot, 1)));
-  CU(dalloc(&c.el, std::max(c.EDtot, 1)));
-  CU(dalloc(&c.tc, std::max(c.ETtot, 1)));
-  CU(dalloc(&c.tn, std::max(c.ETtot, 1)));
-  CU(dalloc(&c.tl, std::max(c.ETtot, 1)));
-  CU(dalloc(&c.e64, (size_t)std::max(c.EDtot, 1) * 4));
-  CU(dalloc(&c.dcdd, (size_t)std::max(c.EDtot, 1) * 2 * D));
-  CU(dalloc(&c.tgt64, h_tgt64.size()));
-  CU(dalloc(&c.elm, h_elm.size()));
-  CU(dalloc(&c.pt_pair, c.NPtot));
-  CU(dalloc(&c.adj_ptr, c.NPtot + 1));
-  CU(dalloc(&c.adj, std::max<size_t>(h_adj.size(), 1)));
-  CU(dalloc(&c.reg_part, (size_t)c.T * c.ngrp_tot));
-  CU(dalloc(&c.vfd_part, std::max(c.netile_tot, 1)));
-  CU(dalloc(&c.f_dev, num));
-  CU(dalloc(&c.pt_items, std::max(c.n_pt_items, 1)));
-  CU(dalloc(&c.el_items, std::max(c.n_el_items, 1)));
-  CU(dalloc(&c.chunk_pair, c.nchunk_tot));
-  CU(dalloc(&c.XT, c.nvar));
-  CU(dalloc(&c.GT, c.nvar));
-  CU(dalloc(&c.part[0], (size_t)c.nchunk_tot * 3));
-  CU(dalloc(&c.part[1], (size_t)c.nchunk_tot * 3));
-
-  CU(cudaMemcpy(c.qs, h_qs.data(), sizeof(float4) * c.NPtot, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(c.q64, h_q64.data(), sizeof(double) * h_q64.size(), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(c.pt_pair, h_ptpair.data(), sizeof(int) * c.NPtot, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(c.elm, h_elm.data(), sizeof(int4) * h_elm.size(), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(c.tc, h_tc.data(), sizeof(float4) * h_tc.size(), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(c.tn, h_tn.data(), sizeof(float4) * h_tn.size(), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(c.tl, h_tl.data(), sizeof(float4) * h_tl.size(), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(c.tgt64, h_tgt64.data(), sizeof(double) * h_tgt64.size(), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(c.adj_ptr, h_adjptr.data(), sizeof(int) * h_adjptr.size(), cudaMemcpyHostToDevice));
-  if (!h_adj.empty())
-    CU(cudaMemcpy(c.adj, h_adj.data(), sizeof(int4) * h_adj.size(), cudaMemcpyHostToDevice));
-  if (c.n_pt_items)
-    CU(cudaMemcpy(c.pt_items, pti.data(), sizeof(int2) * pti.size(), cudaMemcpyHostToDevice));
-  if (c.n_el_items)
-    CU(cudaMemcpy(c.el_items, eli.data(), sizeof(int2) * eli.size(), cudaMemcpyHostToDevice));
-  CU(dalloc(&c.units, std::max(c.n_units, 1)));
-  CU(cudaMemcpy(c.units, uni.data(), sizeof(int2) * uni.size(), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(c.chunk_pair, h_chunk.data(), sizeof(int) * h_chunk.size(), cudaMemcpyHostToDevice));
-
+  // ---- device memory (stream-ordered on the context's stream)
   if (cf.stream) {
     c.stream = (cudaStream_t)cf.stream;
   } else {
     CU(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
     c.own_stream = true;
   }
+  CU(dalloc(c.stream, &c.pd, num));
+  CU(dalloc(c.stream, &c.act, num));
+  CU(dalloc(c.stream, &c.st, num));
+  CU(dalloc(c.stream, &c.qs, (size_t)(c.T + 1) * c.NPtot));
+  CU(dalloc(c.stream, &c.as, (size_t)c.T * c.NPtot));
+  CU(dalloc(c.stream, &c.us, (size_t)2 * c.NPtot));
+  CU(dalloc(c.stream, &c.ls, (size_t)2 * c.NPtot));
+  CU(dalloc(c.stream, &c.q64, (size_t)(c.T + 1) * c.NPtot * D));
+  CU(dalloc(c.stream, &c.p64, (size_t)c.NPtot * D));
+  CU(dalloc(c.stream, &c.ec, std::max(c.EDtot, 1)));
+  CU(dalloc(c.stream, &c.en, std::max(c.EDtot, 1)));
+  CU(dalloc(c.stream, &c.el, std::max(c.EDtot, 1)));
+  CU(dalloc(c.stream, &c.tc, std::max(c.ETtot, 1)));
+  CU(dalloc(c.stream, &c.tn, std::max(c.ETtot, 1)));
+  CU(dalloc(c.stream, &c.tl, std::max(c.ETtot, 1)));
+  CU(dalloc(c.stream, &c.e64, (size_t)std::max(c.EDtot, 1) * 4));
+  CU(dalloc(c.stream, &c.dcdd, (size_t)std::max(c.EDtot, 1) * 2 * D));
+  CU(dalloc(c.stream, &c.tgt64, h_tgt64.size()));
+  CU(dalloc(c.stream, &c.elm, h_elm.size()));
+  CU(dalloc(c.stream, &c.pt_pair, c.NPtot));
+  CU(dalloc(c.stream, &c.adj_ptr, c.NPtot + 1));
+  CU(dalloc(c.stream, &c.adj, std::max<size_t>(h_adj.size(), 1)));
+  CU(dalloc(c.stream, &c.reg_part, (size_t)c.T * c.ngrp_tot));
+  CU(dalloc(c.stream, &c.vfd_part, std::max(c.netile_tot, 1)));
+  CU(dalloc(c.stream, &c.f_dev, num));
+  CU(dalloc(c.stream, &c.pt_items, std::max(c.n_pt_items, 1)));
+  CU(dalloc(c.stream, &c.el_items, std::max(c.n_el_items, 1)));
+  CU(dalloc(c.stream, &c.chunk_pair, c.nchunk_tot));
+  CU(dalloc(c.stream, &c.XT, c.nvar));
+  CU(dalloc(c.stream, &c.GT, c.nvar));
+  CU(dalloc(c.stream, &c.part[0], (size_t)c.nchunk_tot * 3));
+  CU(dalloc(c.stream, &c.part[1], (size_t)c.nchunk_tot * 3));
+
+  CU(cudaMemcpyAsync(c.qs, h_qs.data(), sizeof(float4) * c.NPtot,
+                     cudaMemcpyHostToDevice, c.stream));
+  CU(cudaMemcpyAsync(c.q64, h_q64.data(), sizeof(double) * h_q64.size(),
+                     cudaMemcpyHostToDevice, c.stream));
+  CU(cudaMemcpyAsync(c.pt_pair, h_ptpair.data(), sizeof(int) * c.NPtot,
+                     cudaMemcpyHostToDevice, c.stream));
+  CU(cudaMemcpyAsync(c.elm, h_elm.data(), sizeof(int4) * h_elm.size(),
+                     cudaMemcpyHostToDevice, c.stream));
+  CU(cudaMemcpyAsync(c.tc, h_tc.data(), sizeof(float4) * h_tc.size(),
+                     cudaMemcpyHostToDevice, c.stream));
+  CU(cudaMemcpyAsync(c.tn, h_tn.data(), sizeof(float4) * h_tn.size(),
+                     cudaMemcpyHostToDevice, c.stream));
+  CU(cudaMemcpyAsync(c.tl, h_tl.data(), sizeof(float4) * h_tl.size(),
+                     cudaMemcpyHostToDevice, c.stream));
+  CU(cudaMemcpyAsync(c.tgt64, h_tgt64.data(), sizeof(double) * h_tgt64.size(),
+                     cudaMemcpyHostToDevice, c.stream));
+  CU(cudaMemcpyAsync(c.adj_ptr, h_adjptr.data(), sizeof(int) * h_adjptr.size(),
+                     cudaMemcpyHostToDevice, c.stream));
+  if (!h_adj.empty())
+    CU(cudaMemcpyAsync(c.adj, h_adj.data(), sizeof(int4) * h_adj.size(),
+                       cudaMemcpyHostToDevice, c.stream));
+  if (c.n_pt_items)
+    CU(cudaMemcpyAsync(c.pt_items, pti.data(), sizeof(int2) * pti.size(),
+                       cudaMemcpyHostToDevice, c.stream));
+  if (c.n_el_items)
+    CU(cudaMemcpyAsync(c.el_items, eli.data(), sizeof(int2) * eli.size(),
+                       cudaMemcpyHostToDevice, c.stream));
+  CU(dalloc(c.stream, &c.units, std::max(c.n_units, 1)));
+  CU(cudaMemcpyAsync(c.units, uni.data(), sizeof(int2) * uni.size(),
+                     cudaMemcpyHostToDevice, c.stream));
+  CU(cudaMemcpyAsync(c.chunk_pair, h_chunk.data(), sizeof(int) * h_chunk.size(),
+                     cudaMemcpyHostToDevice, c.stream));
+
 
   // ---- target self-term, FP64, once
   for (int p = 0; p < num && c.has_vfd; ++p) {
@@ -861,20 +931,20 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
     if (P.Et == 0) continue;
     const int nblk = (P.Et + 255) / 256;
     double *part = nullptr;
-    CU(dalloc(&part, nblk));
+    CU(dalloc(c.stream, &part, nblk));
     const double dw = probs[p].dir_knl_width > 0 ? probs[p].dir_knl_width : 1.0;
     cudaError_t e = c.tt(c, p, part, nblk, probs[p].cen_knl_width, dw);
     std::vector<double> hp(nblk);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hp.data(), part, sizeof(double) * nblk,
                                               cudaMemcpyDeviceToHost, c.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
-    cudaFree(part);
+    cudaFreeAsync(part, c.stream);
     CU(e);
     double tt = 0.0;
     for (double x : hp) tt += x;
     c.hpd[p].tt = tt;
   }
-  CU(cudaMemcpy(c.pd, c.hpd.data(), sizeof(PairDesc) * num, cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(c.pd, c.hpd.data(), sizeof(PairDesc) * num, cudaMemcpyHostToDevice, c.stream));
 
   c.S_shoot = cf.cluster_shoot > 0 ? cf.cluster_shoot : default_cluster(c.n_pt_items);
   c.S_adj = cf.cluster_adjoint > 0 ? cf.cluster_adjoint : default_cluster(c.n_pt_items);
@@ -896,22 +966,23 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
     // batches keep per-step launches, whose 64-row tiles are cheaper per pair
     c.persistent = cap > 0 && (cf.persistent > 0 ||
                                (cf.persistent == 0 && c.n_units <= kPersistAutoUnits * cap));
-    CU(dalloc(&c.sync, 1));
+    CU(dalloc(c.stream, &c.sync, 1));
     if (c.persistent) {
       const HostPlan h = plan_sweeps(uni, c.hpd, cap);
       c.pers_ctas = (int)h.cta_seg.size() - 1;
       c.n_segs = (int)h.segs.size();
       c.n_slots = h.slots;
-      CU(dalloc(&c.segs, c.n_segs));
-      CU(dalloc(&c.cta_seg, h.cta_seg.size()));
-      CU(dalloc(&c.unit_parts, h.unit_parts.size()));
-      CU(dalloc(&c.seg_part, (size_t)std::max(c.n_slots, 1) * kGroup * kPartNA));
-      CU(dalloc(&c.unit_cnt, std::max(c.n_units, 1)));
-      CU(cudaMemcpy(c.segs, h.segs.data(), sizeof(int4) * h.segs.size(), cudaMemcpyHostToDevice));
-      CU(cudaMemcpy(c.cta_seg, h.cta_seg.data(), sizeof(int) * h.cta_seg.size(),
-                    cudaMemcpyHostToDevice));
-      CU(cudaMemcpy(c.unit_parts, h.unit_parts.data(), sizeof(int2) * h.unit_parts.size(),
-                    cudaMemcpyHostToDevice));
+      CU(dalloc(c.stream, &c.segs, c.n_segs));
+      CU(dalloc(c.stream, &c.cta_seg, h.cta_seg.size()));
+      CU(dalloc(c.stream, &c.unit_parts, h.unit_parts.size()));
+      CU(dalloc(c.stream, &c.seg_part, (size_t)std::max(c.n_slots, 1) * kGroup * kPartNA));
+      CU(dalloc(c.stream, &c.unit_cnt, std::max(c.n_units, 1)));
+      CU(cudaMemcpyAsync(c.segs, h.segs.data(), sizeof(int4) * h.segs.size(),
+                         cudaMemcpyHostToDevice, c.stream));
+      CU(cudaMemcpyAsync(c.cta_seg, h.cta_seg.data(), sizeof(int) * h.cta_seg.size(),
+                         cudaMemcpyHostToDevice, c.stream));
+      CU(cudaMemcpyAsync(c.unit_parts, h.unit_parts.data(), sizeof(int2) * h.unit_parts.size(),
+                         cudaMemcpyHostToDevice, c.stream));
     }
     int bc = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bc, lbfgs_cycle_kernel, kVecThreads, 0) ==
@@ -942,7 +1013,8 @@ static cudaError_t reset_sync(lddmm_ctx &c) {
 static int check_sync(lddmm_ctx &c) {
   if (!c.persistent) return 0;
   unsigned int w[2] = {0, 0};
-  CU(cudaMemcpy(w, c.sync, sizeof(w), cudaMemcpyDeviceToHost));
+  CU(cudaMemcpyAsync(w, c.sync, sizeof(w), cudaMemcpyDeviceToHost, c.stream));
+  CU(cudaStreamSynchronize(c.stream));
   if (w[1]) {
     set_err("a persistent sweep's grid barrier timed out at step %u (the grid was not "
             "co-resident)", w[1] - 1);
@@ -1059,7 +1131,7 @@ extern "C" int lddmm_shoot(lddmm_ctx *ctx, const double *alp, double *nde_stk, d
   CU(launch_set_active(c, c.P));
   CU(load_trial(c, alp, true));
   double *vlc = nullptr;
-  CU(dalloc(&vlc, (size_t)c.T * c.NPtot * D));
+  CU(dalloc(c.stream, &vlc, (size_t)c.T * c.NPtot * D));
   cudaError_t e = reset_sync(c);
   if (e == cudaSuccess && c.persistent) e = c.shoot_all(c, vlc);
   for (int t = 0; t < c.T && e == cudaSuccess && !c.persistent; ++t)
@@ -1070,7 +1142,7 @@ extern "C" int lddmm_shoot(lddmm_ctx *ctx, const double *alp, double *nde_stk, d
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(hv.data(), vlc, sizeof(double) * hv.size(), cudaMemcpyDeviceToHost, c.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
-  cudaFree(vlc);
+  cudaFreeAsync(vlc, c.stream);
   CU(e);
   {
     const int rc = check_sync(c);
@@ -1099,22 +1171,22 @@ extern "C" int lddmm_shoot(lddmm_ctx *ctx, const double *alp, double *nde_stk, d
 
 static cudaError_t ensure_lbfgs_buffers(lddmm_ctx &c, int m, int rec_cap) {
   if (!c.X) {
-    CUE(dalloc(&c.X, c.nvar));
-    CUE(dalloc(&c.G, c.nvar));
-    CUE(dalloc(&c.Dv, c.nvar));
-    CUE(dalloc(&c.Qv, c.nvar));
+    CUE(dalloc(c.stream, &c.X, c.nvar));
+    CUE(dalloc(c.stream, &c.G, c.nvar));
+    CUE(dalloc(c.stream, &c.Dv, c.nvar));
+    CUE(dalloc(c.stream, &c.Qv, c.nvar));
   }
   if (c.m_alloc < m) {
-    dfree(c.Sh);
-    dfree(c.Yh);
-    CUE(dalloc(&c.Sh, (size_t)m * c.nvar));
-    CUE(dalloc(&c.Yh, (size_t)m * c.nvar));
+    dfree(c.Sh, c.stream);
+    dfree(c.Yh, c.stream);
+    CUE(dalloc(c.stream, &c.Sh, (size_t)m * c.nvar));
+    CUE(dalloc(c.stream, &c.Yh, (size_t)m * c.nvar));
     c.m_alloc = m;
     c.graph_valid = false;
   }
   if (c.rec_cap < rec_cap) {
-    dfree(c.rec);
-    CUE(dalloc(&c.rec, (size_t)c.P * rec_cap * 4));
+    dfree(c.rec, c.stream);
+    CUE(dalloc(c.stream, &c.rec, (size_t)c.P * rec_cap * 4));
     c.rec_cap = rec_cap;
     c.graph_valid = false;
   }
@@ -1223,7 +1295,7 @@ static bool build_loop_graph(lddmm_ctx &c, const OptParams &o, int max_cycles) {
     c.loop_exec = nullptr;
   }
   c.loop_valid = false;
-  if (!c.cyc && dalloc(&c.cyc, 1) != cudaSuccess) return false;
+  if (!c.cyc && dalloc(c.stream, &c.cyc, 1) != cudaSuccess) return false;
   cudaGraph_t g = nullptr;
   if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
   bool ok = false;
@@ -1384,7 +1456,9 @@ static int lbfgs_run(lddmm_ctx &c, const lddmm_opt *opt, const double *alp, bool
   }
   if (opt->vbs_flg) {
     std::vector<double> rec((size_t)c.P * c.rec_cap * 4);
-    CU(cudaMemcpy(rec.data(), c.rec, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost));
+    CU(cudaMemcpyAsync(rec.data(), c.rec, sizeof(double) * rec.size(), cudaMemcpyDeviceToHost,
+                       c.stream));
+    CU(cudaStreamSynchronize(c.stream));
     for (int p = 0; p < c.P; ++p)
       print_table(c, p, rec, std::min(hs[p].iters + 1, c.rec_cap));
   }
@@ -1412,11 +1486,14 @@ extern "C" int lddmm_lbfgs_device(lddmm_ctx *ctx, const lddmm_opt *opt, double *
 extern "C" int lddmm_lbfgs_trace(const lddmm_ctx *ctx, int pair, double *rows4, int cap) {
   if (!ctx || pair < 0 || pair >= ctx->P || !rows4 || !ctx->rec) return LDDMM_ERR_ARG;
   PairState s;
-  if (cudaMemcpy(&s, ctx->st + pair, sizeof(s), cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (cudaMemcpyAsync(&s, ctx->st + pair, sizeof(s), cudaMemcpyDeviceToHost, ctx->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess)
     return LDDMM_ERR_CUDA;
   const int n = std::min({s.iters + 1, ctx->rec_cap, cap});
-  if (cudaMemcpy(rows4, ctx->rec + (size_t)pair * ctx->rec_cap * 4, sizeof(double) * 4 * n,
-                 cudaMemcpyDeviceToHost) != cudaSuccess)
+  if (cudaMemcpyAsync(rows4, ctx->rec + (size_t)pair * ctx->rec_cap * 4, sizeof(double) * 4 * n,
+                      cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess)
     return LDDMM_ERR_CUDA;
   return n;
 }
@@ -1424,7 +1501,9 @@ extern "C" int lddmm_lbfgs_trace(const lddmm_ctx *ctx, int pair, double *rows4, 
 extern "C" int lddmm_ctx_timeline(const lddmm_ctx *ctx, double *us6) {
   if (!ctx || !us6 || !ctx->sync) return LDDMM_ERR_ARG;
   StepSync h;
-  if (cudaMemcpy(&h, ctx->sync, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) {
+  if (cudaMemcpyAsync(&h, ctx->sync, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
     set_err("lddmm_ctx_timeline: %s", cudaGetErrorString(cudaGetLastError()));
     return LDDMM_ERR_CUDA;
   }
@@ -1643,8 +1722,9 @@ extern "C" int lddmm_dq_kernel(int dim, int n, const double *q, const double *l,
     hr[P.pt_off + i] = make_float4(b[0], b[1], b[2], 0.0f);
   }
   double *pd = nullptr;
-  CU(dalloc(&pd, (size_t)c.NPtot * dim));
-  std::unique_ptr<double, cudaError_t (*)(void *)> pguard(pd, cudaFree);
+  CU(dalloc(c.stream, &pd, (size_t)c.NPtot * dim));
+  DevBuf<double> pguard(c.stream);
+  pguard.p = pd;
   CU(cudaMemsetAsync(c.us, 0, sizeof(float4) * c.NPtot, c.stream));
   CU(cudaMemcpyAsync(c.ls, hl.data(), sizeof(float4) * c.NPtot, cudaMemcpyHostToDevice, c.stream));
   CU(cudaMemcpyAsync(c.as, hr.data(), sizeof(float4) * c.NPtot, cudaMemcpyHostToDevice, c.stream));
@@ -1684,8 +1764,9 @@ extern "C" int lddmm_varifold(const lddmm_problem *prob, const double *nde, doub
   CU(cudaMemsetAsync(c.reg_part, 0, sizeof(double) * c.T * c.ngrp_tot, c.stream));
   CU(launch_set_active(c, 1));
   double *dqd = nullptr;
-  CU(dalloc(&dqd, (size_t)c.NPtot * D));
-  std::unique_ptr<double, cudaError_t (*)(void *)> g2(dqd, cudaFree);
+  CU(dalloc(c.stream, &dqd, (size_t)c.NPtot * D));
+  DevBuf<double> g2(c.stream);
+  g2.p = dqd;
   if (c.has_vfd) {
     CU(launch_geometry(c, q64T));
     CU(c.varifold(c));

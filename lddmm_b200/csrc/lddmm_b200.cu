@@ -190,7 +190,7 @@ struct lddmm_ctx {
   cudaError_t (*adjoint_all)(lddmm_ctx &, double *g) = nullptr;
   int (*pers_blocks)(int which) = nullptr;  // resident CTAs per SM of the persistent kernels
   cudaError_t (*varifold)(lddmm_ctx &) = nullptr;
-  cudaError_t (*tt)(lddmm_ctx &, int p, double *part, int nblk, double cw, double dw) = nullptr;
+  cudaError_t (*tt)(lddmm_ctx &, int p, double *part, dim3 grid, double cw, double dw) = nullptr;
 
   ~lddmm_ctx();
 };
@@ -380,9 +380,9 @@ static cudaError_t varifold_impl(lddmm_ctx &c) {
 }
 
 template <int D, char CT, char DT>
-static cudaError_t tt_impl(lddmm_ctx &c, int p, double *part, int nblk, double cw, double dw) {
+static cudaError_t tt_impl(lddmm_ctx &c, int p, double *part, dim3 grid, double cw, double dw) {
   const PairDesc &P = c.hpd[p];
-  target_self_kernel<D, CT, DT><<<nblk, 256, 0, c.stream>>>(c.tgt64 + (size_t)P.tg_off * 8, P.Et,
+  target_self_kernel<D, CT, DT><<<grid, 256, 0, c.stream>>>(c.tgt64 + (size_t)P.tg_off * 8, P.Et,
                                                             cw, dw, part);
   return cudaGetLastError();
 }
@@ -925,24 +925,40 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
                      cudaMemcpyHostToDevice, c.stream));
 
 
-  // ---- target self-term, FP64, once
-  for (int p = 0; p < num && c.has_vfd; ++p) {
-    const PairDesc &P = c.hpd[p];
-    if (P.Et == 0) continue;
-    const int nblk = (P.Et + 255) / 256;
+  // ---- target self-term, FP64, once: every pair's blocks launched, one read-back
+  if (c.has_vfd) {
+    int sms = 0;
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c.device));
+    std::vector<dim3> grid(num);
+    std::vector<size_t> off(num + 1, 0);
+    for (int p = 0; p < num; ++p) {
+      const int Et = c.hpd[p].Et;
+      const int nblk = (Et + 255) / 256;
+      // j chunks so that a pair alone fills about four CTAs per SM
+      const int ny = Et > 0 ? std::max(1, std::min(64, (4 * sms + nblk - 1) / nblk)) : 0;
+      grid[p] = dim3((unsigned)nblk, (unsigned)ny);
+      off[p + 1] = off[p] + (size_t)nblk * ny;
+    }
     double *part = nullptr;
-    CU(dalloc(c.stream, &part, nblk));
-    const double dw = probs[p].dir_knl_width > 0 ? probs[p].dir_knl_width : 1.0;
-    cudaError_t e = c.tt(c, p, part, nblk, probs[p].cen_knl_width, dw);
-    std::vector<double> hp(nblk);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(hp.data(), part, sizeof(double) * nblk,
-                                              cudaMemcpyDeviceToHost, c.stream);
+    CU(dalloc(c.stream, &part, std::max<size_t>(off[num], 1)));
+    cudaError_t e = cudaSuccess;
+    for (int p = 0; p < num && e == cudaSuccess; ++p) {
+      if (c.hpd[p].Et == 0) continue;
+      const double dw = probs[p].dir_knl_width > 0 ? probs[p].dir_knl_width : 1.0;
+      e = c.tt(c, p, part + off[p], grid[p], probs[p].cen_knl_width, dw);
+    }
+    std::vector<double> hp(std::max<size_t>(off[num], 1));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(hp.data(), part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost,
+                          c.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
     cudaFreeAsync(part, c.stream);
     CU(e);
-    double tt = 0.0;
-    for (double x : hp) tt += x;
-    c.hpd[p].tt = tt;
+    for (int p = 0; p < num; ++p) {
+      double tt = 0.0;
+      for (size_t k = off[p]; k < off[p + 1]; ++k) tt += hp[k];
+      c.hpd[p].tt = tt;
+    }
   }
   CU(cudaMemcpyAsync(c.pd, c.hpd.data(), sizeof(PairDesc) * num, cudaMemcpyHostToDevice, c.stream));
 

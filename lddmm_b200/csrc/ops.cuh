@@ -578,17 +578,21 @@ __global__ void objective_kernel(const PairDesc *__restrict__ pd, const int *__r
 }
 
 // Target self-term in FP64, once per context (the constant third double loop of
-// dqVf_Kernel, Cpp/src/varifold3D.cpp:334-354).  Block partials per (pair, i-block).
+// dqVf_Kernel, Cpp/src/varifold3D.cpp:334-354).  Grid (i blocks, j chunks): block
+// (x, y) sums rows [256 x, 256 x + 256) against columns [Et y / ny, Et (y + 1) / ny)
+// and writes one partial, part[y * gridDim.x + x]; the host adds them in index order.
 template <int D, char CT, char DT>
 __global__ void target_self_kernel(const double *__restrict__ tgt, int Et, double cw, double dw,
                                    double *part) {
   __shared__ double scr[32];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j0 = (int)((long long)Et * blockIdx.y / gridDim.y);
+  const int j1 = (int)((long long)Et * (blockIdx.y + 1) / gridDim.y);
   double s = 0.0;
   if (i < Et) {
     const double *ti = tgt + (size_t)i * 8;
-    const double w2 = cw * cw, ow2 = 2.0 / (dw * dw);
-    for (int j = 0; j < Et; ++j) {
+    const double iw2 = 1.0 / (cw * cw), ow2 = 2.0 / (dw * dw);
+    for (int j = j0; j < j1; ++j) {
       const double *tj = tgt + (size_t)j * 8;
       double r2 = 0.0, ang = 0.0;
       for (int d = 0; d < D; ++d) {
@@ -596,17 +600,18 @@ __global__ void target_self_kernel(const double *__restrict__ tgt, int Et, doubl
         r2 += x * x;
         ang += ti[3 + d] * tj[3 + d];
       }
-      const double k = (CT == 'G') ? exp(-r2 / w2) : 1.0 / (1.0 + r2 / w2);
+      const double k = (CT == 'G') ? exp(-r2 * iw2) : 1.0 / (1.0 + r2 * iw2);
       double b;
       if (DT == 'B') b = ang * ang;
       else if (DT == 'L') b = ang;
       else if (DT == 'O') b = exp((ang - 1.0) * ow2);
       else b = exp((ang * ang - 1.0) * ow2);
-      s += k * b * ti[6] * tj[6];
+      s += k * b * tj[6];
     }
+    s *= ti[6];
   }
   const double tot = block_sum(s, scr);
-  if (threadIdx.x == 0) part[blockIdx.x] = tot;
+  if (threadIdx.x == 0) part[blockIdx.y * gridDim.x + blockIdx.x] = tot;
 }
 
 }  // namespace lddmm

@@ -37,6 +37,7 @@ UNIT = "registrations/s"
 WORKLOAD = "sphere2cube: icosphere 2562 v / 5120 t -> cube 12288 t, Matern nu=3/2 w=0.4, " \
            "varifold G(0.15) x Binet, T=20, L-BFGS m=5, <=500 iterations"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+BATCH_PAIRS = 8  # registrations in the batched-form measurement
 
 # The FP64 registration of this workload (CPU oracle, 500 iterations; generator
 # tests/golden/make_c2_reference.py): its objective is what a registration has to
@@ -314,6 +315,34 @@ def run_ours(args):
            + P.tgt_dir.nbytes + P.tgt_vol.nbytes)
     d2h = out.nbytes
 
+    # batched form: BATCH_PAIRS copies of the workload registered together in one
+    # context (one launch per sweep for all pairs), device-resident, same options
+    batched = None
+    if rank == 0:
+        with api.Context([P] * BATCH_PAIRS, stream=stream.cuda_stream, device=local) as cb:
+            d_b = torch.zeros(cb.var_total, dtype=torch.float64, device="cuda")
+            res_b = (_lib.Result * BATCH_PAIRS)()
+
+            def batch_registration():
+                d_b.zero_()
+                _lib.check(min(_lib.lib.lddmm_lbfgs_device(cb.handle, C.byref(opt),
+                                                           C.c_void_p(d_b.data_ptr()), res_b), 0))
+
+            for _ in range(2):
+                batch_registration()
+            torch.cuda.synchronize()
+            b0 = torch.cuda.Event(enable_timing=True)
+            b1 = torch.cuda.Event(enable_timing=True)
+            flush.zero_()
+            b0.record(stream)
+            batch_registration()
+            b1.record(stream)
+            torch.cuda.synchronize()
+            b_ms = b0.elapsed_time(b1)
+            batched = {"pairs": BATCH_PAIRS, "registrations_per_s": BATCH_PAIRS / (b_ms * 1e-3),
+                       "ms_per_batch": b_ms,
+                       "iters": [r.iters for r in res_b], "status": [r.status for r in res_b]}
+
     # roofline of the dominant sweep: live per-launch timing (CUDA events on the
     # context stream) of one evaluation at the returned point
     sweeps = ctx.time_sweeps(reps=5)
@@ -393,6 +422,7 @@ def run_ours(args):
                     "call": "lddmm_LDDMM (host buffers; context set-up inside)"},
             "gpu_launches": launches,
             "clocks": clocks,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

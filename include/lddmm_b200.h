@@ -236,6 +236,55 @@ int lddmm_fp32_peak(int device, double *tflops);
  * shooting step, the fused adjoint step and the varifold pair of the given kinds. */
 double lddmm_flops_per_pair(int sweep, int dim, int knl_order, char cen_type, char dir_type);
 
+/* ---------------------------------------------------------------------------------
+ * Learned warm start.  No counterpart in the reference: the reference's LBFGS starts
+ * from the momenta it is given (LDDMM.m passes zeros).  A small per-point network,
+ * trained on momenta that the plain method produced, predicts a registration's
+ * initial momenta from the source landmarks and the target's varifold; the plain
+ * L-BFGS then runs from that start as usual.  Network: per target triangle
+ * (centre, unit normal, area * Et / (4 pi)) -> 64 (GELU) -> 64, max-pooled over the
+ * triangles to g; per source landmark (q_i, g) -> 256 (GELU) -> 256 (GELU) -> 3T, the
+ * momenta of the T steps divided by label_scale.  BF16 operands, FP32 accumulation on
+ * the tensor cores (tcgen05), FP32 master weights, Adam.  All buffers are device
+ * pointers on the context's stream; calls are synchronous.
+ * --------------------------------------------------------------------------------- */
+typedef struct lddmm_ws lddmm_ws;
+
+/* Creates a network for one source shape (n_src landmarks, src_nde n_src x 3, C++
+ * layout), time_steps T (3T <= 256 outputs per landmark), batches of up to batch_max
+ * pairs with up to tri_max target triangles, labels divided by label_scale, initial
+ * weights uniform(+-1/sqrt(fan-in)) from `seed`.  stream: cudaStream_t or NULL (own). */
+int lddmm_ws_create(int n_src, const double *src_nde, int time_steps, int batch_max,
+                    int tri_max, double label_scale, unsigned long long seed, void *stream,
+                    lddmm_ws **out);
+void lddmm_ws_destroy(lddmm_ws *ws);
+const char *lddmm_ws_last_error(void);
+/* Number of FP32 parameters: per layer (target 1, target 2, point 1, point 2, point 3)
+ * Wt[out][in] then b[out], dimensions padded to multiples of 16 (7 -> 16, 67 -> 80,
+ * 3T -> round16(3T)); padded entries are zero. */
+long long lddmm_ws_num_params(const lddmm_ws *ws);
+/* Copies the flat parameter vector to (set = 0) or from (set != 0) host memory. */
+int lddmm_ws_params(lddmm_ws *ws, float *host, int set);
+/* Mean squared error of `pairs` pairs and its gradient (host, num_params floats; may be
+ * NULL) without updating the weights.  d_tri7: pairs x tri_num x 7 FP32 target
+ * features; d_labels: pairs x n_src x 3T FP32 momenta, label[p][i][3t + d] =
+ * alpha_p[(t n_src + i) 3 + d]. */
+int lddmm_ws_grad(lddmm_ws *ws, const float *d_tri7, int pairs, int tri_num,
+                  const float *d_labels, float *grad_host, double *loss);
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) of learning rate lr on one batch. */
+int lddmm_ws_train_step(lddmm_ws *ws, const float *d_tri7, int pairs, int tri_num,
+                        const float *d_labels, double lr, double *loss);
+/* Predicted momenta of `pairs` pairs in the variable layout (pairs x T x n_src x 3,
+ * FP64), ready as the initial point of lddmm_lbfgs_device. */
+int lddmm_ws_predict(lddmm_ws *ws, const float *d_tri7, int pairs, int tri_num,
+                     double *d_alpha);
+/* The network's BF16 tensor-core GEMM on its own: C[m x n] (FP32, leading dimension
+ * ldc) = A[m x k] . B[n x k]^T, A and B BF16 row-major with k contiguous; n = 16..256
+ * in steps of 16, k a multiple of 16, lda and ldb multiples of 8.  Asynchronous on
+ * `stream`. */
+int lddmm_ws_gemm_bf16(const void *d_a, long long lda, const void *d_b, long long ldb, int m,
+                       int n, int k, float *d_c, long long ldc, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,6 +24,9 @@ EXPORTS = [
     "lddmm_elm_ifo", "lddmm_multiply_kernel", "lddmm_dq_kernel", "lddmm_varifold",
     "lddmm_flops_per_pair", "lddmm_ctx_time_sweeps", "lddmm_ctx_counters",
     "lddmm_fp32_peak", "lddmm_multiply_kernel_noalloc", "lddmm_ctx_timeline",
+    "lddmm_ws_create", "lddmm_ws_destroy", "lddmm_ws_last_error", "lddmm_ws_num_params",
+    "lddmm_ws_params", "lddmm_ws_grad", "lddmm_ws_train_step", "lddmm_ws_predict",
+    "lddmm_ws_gemm_bf16",
 ]
 
 ERRORS = {
@@ -107,6 +110,23 @@ def _load():
     L.lddmm_ctx_timeline.argtypes = [C.c_void_p, _dp]
     L.lddmm_multiply_kernel_noalloc.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                                 C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+    # learned warm start
+    _fp = C.POINTER(C.c_float)
+    L.lddmm_ws_create.argtypes = [C.c_int, _dp, C.c_int, C.c_int, C.c_int, C.c_double,
+                                  C.c_ulonglong, C.c_void_p, C.POINTER(C.c_void_p)]
+    L.lddmm_ws_destroy.argtypes = [C.c_void_p]
+    L.lddmm_ws_destroy.restype = None
+    L.lddmm_ws_last_error.restype = C.c_char_p
+    L.lddmm_ws_num_params.argtypes = [C.c_void_p]
+    L.lddmm_ws_num_params.restype = C.c_longlong
+    L.lddmm_ws_params.argtypes = [C.c_void_p, _fp, C.c_int]
+    L.lddmm_ws_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, _fp, _dp]
+    L.lddmm_ws_train_step.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                      C.c_double, _dp]
+    L.lddmm_ws_predict.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    L.lddmm_ws_gemm_bf16.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong,
+                                     C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_longlong,
+                                     C.c_void_p]
     return L
 
 
@@ -117,6 +137,13 @@ def check(rc: int) -> int:
     """Raise LddmmError for negative return codes; pass line-search codes through."""
     if rc < 0:
         raise LddmmError(rc, lib.lddmm_last_error().decode(errors="replace"))
+    return rc
+
+
+def check_ws(rc: int) -> int:
+    """check() for the warm-start entry points (their own error message)."""
+    if rc < 0:
+        raise LddmmError(rc, lib.lddmm_ws_last_error().decode(errors="replace"))
     return rc
 
 

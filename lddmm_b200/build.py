@@ -3,7 +3,7 @@
     python -m lddmm_b200.build            # or: python lddmm_b200/build.py
 
 One nvcc invocation over lddmm_b200/csrc/lddmm_b200.cu (which includes the kernel
-headers), static CUDA runtime, no fast-math (the approximate MUFU instructions
+headers) and lddmm_b200/csrc/warmstart.cu (the warm-start network), static CUDA runtime, no fast-math (the approximate MUFU instructions
 used in the pair loops are written explicitly; everything else keeps IEEE FP32/FP64).
 """
 from __future__ import annotations
@@ -45,7 +45,8 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
            "-cudart", "static", "-Xptxas", "-v" if verbose else "-O3",
            "-I", os.path.join(os.path.dirname(HERE), "include"),
-           os.path.join(CSRC, "lddmm_b200.cu"), "-o", OUT + ".tmp"]
+           os.path.join(CSRC, "lddmm_b200.cu"), os.path.join(CSRC, "warmstart.cu"),
+           "-o", OUT + ".tmp"]
     if extra:
         cmd[1:1] = list(extra)
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -1,0 +1,246 @@
+// BF16 GEMM on the 5th-generation tensor cores (tcgen05.mma, accumulator in TMEM) for
+// the warm-start network.  No counterpart in the reference.
+//
+//   C[M x N] = A[M x K] . B[N x K]^T      A, B: BF16, K-major (K contiguous); C: FP32
+//
+// One CTA of 4 warps per 128-row tile of C and per K split (blockIdx.y); N <= 256 is
+// one tile (one tcgen05.mma of shape 128 x N x 16 per 16 elements of K).  Operands are
+// staged K-chunk by K-chunk (kKC elements) into shared memory in the canonical
+// K-major layout without swizzle: "core matrices" of 8 rows x 16 bytes, core (g, c)
+// (row group g, 8-element K group c) at byte (g * kKC / 8 + c) * 128, so the leading
+// byte offset (next K group) is 128 and the stride byte offset (next row group) is
+// kKC * 16.  Thread 0 issues the MMAs of a chunk and commits them to an mbarrier; the
+// CTA waits on it (bounded) before restaging.  The epilogue reads the accumulator
+// with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = rows of the tile) and applies
+// bias / GELU / GELU' and writes FP32, BF16 and transposed BF16 outputs as asked.
+//
+// Shared-memory and instruction descriptor bit layouts follow the PTX ISA
+// (tcgen05 "Shared memory descriptor", "Instruction descriptor" for kind::f16).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cstdint>
+
+namespace lddmm {
+namespace tc {
+
+constexpr int kTileM = 128;
+constexpr int kKC = 64;                        // K elements staged per chunk
+constexpr int kGemmThreads = 128;
+constexpr unsigned int kMbarSpin = 1u << 24;   // bounded wait on the MMA barrier
+
+enum Epilogue : int {
+  kEpiNone = 0,   // out = acc (+ bias)
+  kEpiGelu = 1,   // pre = acc + bias (stored if asked), out = gelu(pre)
+  kEpiDGelu = 2,  // out = acc * gelu'(pre_in)
+};
+
+struct GemmArgs {
+  const __nv_bfloat16 *A;
+  long long lda;  // A[m][k] = A[m * lda + k], m < M
+  const __nv_bfloat16 *B;
+  long long ldb;  // B[n][k] = B[n * ldb + k], n < N
+  int M, N, K;    // N: multiple of 16, <= 256 (the MMA shape); K: multiple of 16
+  int n_valid;    // columns written (<= N)
+  int k_split;    // K elements per blockIdx.y (multiple of kKC)
+  int epi;
+  const float *bias;        // [n_valid] or null
+  const float *pre_in;      // kEpiDGelu: [M][ld_pre_in]
+  long long ld_pre_in;
+  float *out;               // FP32 [M][ldo] (+ blockIdx.y * split_stride) or null
+  long long ldo, split_stride;
+  float *pre_out;           // kEpiGelu: FP32 pre-activation [M][ld_pre_out] or null
+  long long ld_pre_out;
+  __nv_bfloat16 *out_bf;    // BF16 [M][ldb_out] or null
+  long long ldb_out;
+  __nv_bfloat16 *out_bt;    // BF16 transposed [n][ldt_out] (column m) or null
+  long long ldt_out;
+  unsigned int *error;      // set to 1 when the MMA barrier wait gave up
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor: start address >> 4 (bits 0-13), leading byte offset
+// >> 4 (16-29), stride byte offset >> 4 (32-45), version 1 (46-47), base offset 0,
+// layout type 0 = no swizzle (61-63).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor, kind::f16: F32 accumulator (bits 4-5 = 1), A and B BF16
+// (7-9 = 1, 10-12 = 1), both K-major (15, 16 = 0), N >> 3 (17-22), M >> 4 (24-28).
+__host__ __device__ constexpr uint32_t instr_desc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t *mbar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(mbar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *mbar, uint32_t parity) {
+  const uint32_t a = smem_u32(mbar);
+  for (unsigned int n = 0; n < kMbarSpin; ++n) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ float gelu(float x) {
+  return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f));
+}
+
+__device__ __forceinline__ float gelu_grad(float x) {
+  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) +
+         x * 0.39894228040143268f * __expf(-0.5f * x * x);
+}
+
+// 32 consecutive accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+      "[%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Stage rows [r0, r0 + rows) x K elements [k0, k0 + kKC) of a K-major matrix into the
+// canonical layout at `dst` (rows beyond `rmax` and K beyond `kmax` read as zero).
+__device__ __forceinline__ void stage(unsigned char *dst, const __nv_bfloat16 *src, long long ld,
+                                      int r0, int rows, int rmax, int k0, int kmax) {
+  constexpr int kChunks = kKC / 8;  // 16-byte groups per row
+  for (int i = threadIdx.x; i < rows * kChunks; i += kGemmThreads) {
+    const int r = i / kChunks, c = i - r * kChunks;
+    const int gr = r0 + r, gk = k0 + c * 8;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (gr < rmax && gk < kmax) v = *reinterpret_cast<const uint4 *>(src + gr * ld + gk);
+    *reinterpret_cast<uint4 *>(dst + ((r >> 3) * kChunks + c) * 128 + (r & 7) * 16) = v;
+  }
+}
+
+__global__ void __launch_bounds__(kGemmThreads, 1) gemm_bf16_kernel(GemmArgs g) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char *sA = smem;                                // kTileM x kKC bf16
+  unsigned char *sB = smem + kTileM * kKC * 2;             // N x kKC bf16
+  __shared__ uint64_t s_mbar;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_ok;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * kTileM;
+  const int kb = blockIdx.y * g.k_split, ke = min(g.K, kb + g.k_split);
+  const uint32_t ncols = g.N <= 32 ? 32u : g.N <= 64 ? 64u : g.N <= 128 ? 128u : 256u;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_ok = 1;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+  const uint32_t idesc = instr_desc_bf16(kTileM, g.N);
+  uint32_t phase = 0;
+  bool first = true;
+  for (int k0 = kb; k0 < ke; k0 += kKC) {
+    stage(sA, g.A, g.lda, m0, kTileM, g.M, k0, ke);
+    stage(sB, g.B, g.ldb, 0, g.N, g.N, k0, ke);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+      for (int s = 0; s < kKC / 16; ++s) {
+        // K step s covers K groups 2s and 2s + 1 (start advances by 2 core matrices)
+        const uint64_t da = smem_desc(a0 + s * 256, 128, kKC * 16);
+        const uint64_t db = smem_desc(b0 + s * 256, 128, kKC * 16);
+        mma_bf16(tmem, da, db, idesc, (first && s == 0) ? 0u : 1u);
+      }
+      mma_commit(&s_mbar);
+    }
+    first = false;
+    // every thread waits for the chunk's MMAs before the stage buffers are rewritten
+    if (!mbar_wait(&s_mbar, phase)) {
+      s_ok = 0;
+      if (g.error) atomicExch(g.error, 1u);
+    }
+    phase ^= 1u;
+    __syncthreads();
+    if (!s_ok) break;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (s_ok && !first) {
+    const int m = m0 + warp * 32 + lane;
+    const bool row_ok = m < g.M;
+    float *out = g.out ? g.out + (size_t)blockIdx.y * g.split_stride : nullptr;
+    for (int c0 = 0; c0 < g.N; c0 += 32) {
+      float v[32];
+      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+      if (!row_ok) continue;
+#pragma unroll 4
+      for (int j = 0; j < 32; ++j) {
+        const int n = c0 + j;
+        if (n >= g.n_valid) break;
+        float x = v[j];
+        if (g.bias) x += g.bias[n];
+        if (g.epi == kEpiGelu) {
+          if (g.pre_out) g.pre_out[(size_t)m * g.ld_pre_out + n] = x;
+          x = gelu(x);
+        } else if (g.epi == kEpiDGelu) {
+          x *= gelu_grad(g.pre_in[(size_t)m * g.ld_pre_in + n]);
+        }
+        if (out) out[(size_t)m * g.ldo + n] = x;
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        if (g.out_bf) g.out_bf[(size_t)m * g.ldb_out + n] = h;
+        if (g.out_bt) g.out_bt[(size_t)n * g.ldt_out + m] = h;
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
+
+inline size_t gemm_smem_bytes(int N) { return (size_t)(kTileM + N) * kKC * 2; }
+
+}  // namespace tc
+}  // namespace lddmm

@@ -1,0 +1,252 @@
+"""Learned warm start for L-BFGS (host side).  No counterpart in the reference.
+
+A small network (csrc/warmstart.cu, C ABI ``lddmm_ws_*``) predicts a registration's
+initial momenta from the source landmarks and the target's varifold; the plain
+method then runs from that start as usual and judges the result.  This module holds:
+
+* the workload of the learned part: a 2562-landmark icosphere onto perturbed spheres
+  r = 1 + sum_{l<=6} c_lm Y_lm, c_lm ~ N(0, 0.08^2), 5120 triangles; Gaussian
+  deformation kernel 0.3, varifold Gaussian 0.1 x Binet, T = 10 steps;
+* ``generate``: the training labels, momenta of plain-method registrations run in
+  batches on the device;
+* ``WarmStart``: the network (training steps, prediction, parameters, gradient);
+* ``train`` and ``evaluate`` (cold start from zero vs warm start from the prediction:
+  iterations and evaluations until the objective is within 1e-5 of the cold start's
+  converged objective, and batch wall time to convergence).
+
+Device memory is held in torch tensors; all arithmetic is in the library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+
+import numpy as np
+
+from . import _lib, api, problem, shapes
+from ._lib import check, check_ws, lib
+
+T_STEPS = 10           # time steps of the learned workload (3T = 30 outputs per landmark)
+
+
+def pair(seed: int, src_subdiv: int = 4, tgt_subdiv: int = 4, lmax: int = 6,
+         sigma: float = 0.08, time_num: int = T_STEPS + 1) -> problem.Problem:
+    """Icosphere source (2562 landmarks at subdivision 4) onto a perturbed sphere
+    (5120 triangles at subdivision 4) drawn with `seed`."""
+    V, F = shapes.icosphere(src_subdiv)
+    tv, tf = shapes.star_surface(tgt_subdiv, lmax, sigma, seed)
+    cen, dr, vol = shapes.varifold_of(tv, tf)
+    T = time_num - 1
+    return problem.Problem(V, F, cen, dr, vol, knl_order=-1, knl_width=0.3, time_num=time_num,
+                           time_stp=1.0 / T, cen_type="G", cen_width=0.1, dir_type="B",
+                           dis_wgt=1.0, name=f"warm{seed}")
+
+
+def features(P: problem.Problem) -> np.ndarray:
+    """Target features per triangle: centre, unit normal, area * Et / (4 pi)."""
+    Et = P.tgt_elm_num
+    f = np.empty((Et, 7), dtype=np.float32)
+    f[:, 0:3] = P.tgt_cen
+    f[:, 3:6] = P.tgt_dir
+    f[:, 6] = P.tgt_vol * Et / (4.0 * math.pi)
+    return f
+
+
+def _labels(alpha, n_pairs, T, N):
+    """(pairs, T * N * 3) momenta in the variable layout -> (pairs, N, 3T) labels."""
+    return alpha.view(n_pairs, T, N, 3).permute(0, 2, 1, 3).reshape(n_pairs, N, 3 * T)
+
+
+def register_batch(probs, alp0=None, itr_max=300, tol=1e-12, rel_obj_tol=1e-6, mem_num=5,
+                   trace=False):
+    """L-BFGS of a batch of pairs in one context, device-resident.  Returns (alpha as a
+    (pairs, var) torch float64 tensor, per-pair results, seconds, traces or None)."""
+    import torch
+
+    with api.Context(probs) as ctx:
+        n = len(probs)
+        d = torch.zeros(ctx.var_total, dtype=torch.float64, device="cuda")
+        if alp0 is not None:
+            d.copy_(alp0.reshape(-1))
+        opt = _lib.Opt(itr_max, tol, 1e-4, 0.9, mem_num, 0, rel_obj_tol)
+        res = (_lib.Result * n)()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        check(lib.lddmm_lbfgs_device(ctx.handle, C.byref(opt), C.c_void_p(d.data_ptr()), res))
+        sec = time.perf_counter() - t
+        out = [dict(f=r.fcn, status=r.status, iters=r.iters, evals=r.evals) for r in res]
+        traces = [ctx.trace(p) for p in range(n)] if trace else None
+    return d.view(n, -1), out, sec, traces
+
+
+def generate(seeds, batch=64, itr_max=300, rel_obj_tol=1e-6, log=None, make=pair):
+    """Training data: plain-method registrations of make(seed) for every seed, run
+    `batch` pairs per context.  Returns (tri7 (n, Et, 7) float32, labels (n, N, 3T)
+    float32, source landmarks (N, 3), per-pair results) with tensors on the device."""
+    import torch
+
+    tri, lab, results = [], [], []
+    src = None
+    for k in range(0, len(seeds), batch):
+        probs = [make(s) for s in seeds[k:k + batch]]
+        src = probs[0].ini_nde
+        alpha, res, sec, _ = register_batch(probs, itr_max=itr_max, rel_obj_tol=rel_obj_tol)
+        T, N = probs[0].T, probs[0].nde_num
+        lab.append(_labels(alpha, len(probs), T, N).float())
+        tri.append(torch.from_numpy(np.stack([features(P) for P in probs])).cuda())
+        results += res
+        if log:
+            log(f"generated {k + len(probs)}/{len(seeds)} pairs ({sec:.1f} s for {len(probs)}, "
+                f"median iterations {np.median([r['iters'] for r in res]):.0f})")
+    return torch.cat(tri), torch.cat(lab), src, results
+
+
+class WarmStart:
+    """The network (C ABI lddmm_ws_*): one source shape, T steps, batches of up to
+    `batch_max` pairs with up to `tri_max` target triangles."""
+
+    def __init__(self, src_nde, T, batch_max, tri_max, label_scale, seed=0, stream=None):
+        src = np.ascontiguousarray(src_nde, dtype=np.float64)
+        self.N, self.T = src.shape[0], T
+        h = C.c_void_p()
+        check_ws(lib.lddmm_ws_create(self.N, _lib.dptr(src), T, batch_max, tri_max, label_scale,
+                                     seed, stream, C.byref(h)))
+        self._h = h
+        self.n_params = lib.lddmm_ws_num_params(h)
+
+    def close(self):
+        if self._h:
+            lib.lddmm_ws_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.zeros(self.n_params, dtype=np.float32)
+        check_ws(lib.lddmm_ws_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), 0))
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.n_params
+        check_ws(lib.lddmm_ws_params(self._h, p.ctypes.data_as(C.POINTER(C.c_float)), 1))
+
+    def grad(self, tri7, labels):
+        """(loss, flat gradient) of a batch (device tensors) without an update."""
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = C.c_double()
+        check_ws(lib.lddmm_ws_grad(self._h, C.c_void_p(tri7.data_ptr()), tri7.shape[0],
+                                   tri7.shape[1], C.c_void_p(labels.data_ptr()),
+                                   g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)))
+        return loss.value, g
+
+    def train_step(self, tri7, labels, lr=1e-3):
+        loss = C.c_double()
+        check_ws(lib.lddmm_ws_train_step(self._h, C.c_void_p(tri7.data_ptr()), tri7.shape[0],
+                                         tri7.shape[1], C.c_void_p(labels.data_ptr()), lr,
+                                         C.byref(loss)))
+        return loss.value
+
+    def predict(self, tri7):
+        """Predicted momenta, (pairs, T * N * 3) float64 on the device."""
+        import torch
+
+        out = torch.empty((tri7.shape[0], self.T * self.N * 3), dtype=torch.float64,
+                          device="cuda")
+        check_ws(lib.lddmm_ws_predict(self._h, C.c_void_p(tri7.data_ptr()), tri7.shape[0],
+                                      tri7.shape[1], C.c_void_p(out.data_ptr())))
+        return out
+
+
+def train(ws: WarmStart, tri7, labels, epochs=20, batch=64, lr=1e-3, seed=0, log=None):
+    """Adam over shuffled mini-batches (each pair's rows stay together).  Returns the
+    mean loss of every epoch."""
+    import torch
+
+    n = tri7.shape[0]
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    hist = []
+    for ep in range(epochs):
+        perm = torch.randperm(n, generator=g).cuda()
+        tot, cnt = 0.0, 0
+        for k in range(0, n - batch + 1, batch):
+            idx = perm[k:k + batch]
+            tot += ws.train_step(tri7.index_select(0, idx).contiguous(),
+                                 labels.index_select(0, idx).contiguous(), lr)
+            cnt += 1
+        hist.append(tot / max(cnt, 1))
+        if log:
+            log(f"epoch {ep + 1}/{epochs}: loss {hist[-1]:.4e}")
+    return hist
+
+
+def _time_to(trace, f_target):
+    """(iterations, evaluations) until the iteration table first reaches f_target."""
+    ev = 1
+    for k in range(trace.shape[0]):
+        if k > 0:
+            ev += int(trace[k, 3])
+        if trace[k, 0] <= f_target:
+            return k, ev
+    return None, None
+
+
+def evaluate(ws: WarmStart, seeds, batch=64, itr_max=300, rel_obj_tol=1e-6, rel=1e-5,
+             make=pair):
+    """Cold start (zero momenta) vs warm start (predicted momenta) on the pairs of
+    `seeds`.  Per pair: iterations and objective evaluations until the objective is
+    within `rel` of the cold start's converged objective, and whether the warm run's
+    converged objective is within `rel` of it.  Batch wall times to convergence."""
+    import torch
+
+    rows = []
+    t_cold = t_warm = 0.0
+    for k in range(0, len(seeds), batch):
+        probs = [make(s) for s in seeds[k:k + batch]]
+        tri = torch.from_numpy(np.stack([features(P) for P in probs])).cuda()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        a0 = ws.predict(tri)
+        torch.cuda.synchronize()
+        t_pred = time.perf_counter() - t0
+        _, cold, sc, tc = register_batch(probs, itr_max=itr_max, rel_obj_tol=rel_obj_tol,
+                                         trace=True)
+        _, warm, sw, tw = register_batch(probs, alp0=a0, itr_max=itr_max,
+                                         rel_obj_tol=rel_obj_tol, trace=True)
+        t_cold += sc
+        t_warm += sw + t_pred
+        for p in range(len(probs)):
+            f_ref = cold[p]["f"]
+            target = f_ref * (1.0 + rel) if f_ref >= 0 else f_ref * (1.0 - rel)
+            ic, ec = _time_to(tc[p], target)
+            iw, ew = _time_to(tw[p], target)
+            rows.append(dict(seed=seeds[k + p], f_cold=f_ref, f_warm=warm[p]["f"],
+                             f_start_warm=float(tw[p][0, 0]), f_start_cold=float(tc[p][0, 0]),
+                             it_cold=ic, ev_cold=ec, it_warm=iw, ev_warm=ew,
+                             match=warm[p]["f"] <= target))
+    ok = [r for r in rows if r["ev_warm"] is not None and r["ev_cold"] is not None]
+    return dict(
+        pairs=len(rows),
+        reached=len(ok),
+        matched=sum(r["match"] for r in rows),
+        median_evals_cold=float(np.median([r["ev_cold"] for r in ok])) if ok else None,
+        median_evals_warm=float(np.median([r["ev_warm"] for r in ok])) if ok else None,
+        median_speedup_evals=float(np.median([r["ev_cold"] / r["ev_warm"] for r in ok]))
+        if ok else None,
+        median_iters_cold=float(np.median([r["it_cold"] for r in ok])) if ok else None,
+        median_iters_warm=float(np.median([r["it_warm"] for r in ok])) if ok else None,
+        seconds_cold=t_cold, seconds_warm=t_warm,
+        rows=rows)

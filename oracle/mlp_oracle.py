@@ -1,0 +1,152 @@
+"""CPU oracle of the warm-start network (test infrastructure only).
+
+A numpy restatement of the network and its gradient with the parameter layout of the
+library's flat vector (per layer Wt[out][in] then b[out]; layers: target 1 (16 -> 64),
+target 2 (64 -> 64), point 1 (80 -> 256), point 2 (256 -> 256), point 3
+(256 -> round16(3T))), evaluated in FP64.  With ``bf=True`` it rounds to BF16 (round
+to nearest even) at the points where the CUDA path stores BF16: every GEMM operand
+(inputs, activations, weights, loss gradients), so the two agree up to FP32
+accumulation order; with ``bf=False`` it is the exact FP64 network whose gradient the
+finite-difference test checks.  There is no reference implementation of this part.
+"""
+from __future__ import annotations
+
+import numpy as np
+from scipy.special import erf
+
+TRI_IN, TRI_H, PT_IN, PT_H = 16, 64, 80, 256
+
+
+def round16(n: int) -> int:
+    return (n + 15) // 16 * 16
+
+
+def layer_dims(T: int):
+    """(in, out) of the five layers, padded."""
+    return [(TRI_IN, TRI_H), (TRI_H, TRI_H), (PT_IN, PT_H), (PT_H, PT_H), (PT_H, round16(3 * T))]
+
+
+def num_params(T: int) -> int:
+    return sum(o * i + o for i, o in layer_dims(T))
+
+
+def unpack(params, T):
+    out, off = [], 0
+    for i, o in layer_dims(T):
+        Wt = params[off:off + o * i].reshape(o, i)
+        off += o * i
+        b = params[off:off + o]
+        off += o
+        out.append((Wt, b))
+    return out
+
+
+def to_bf16(x):
+    """Round to the nearest BF16 (ties to even), returned as float64."""
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float32))
+    u = a.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def gelu(x):
+    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+
+
+def gelu_grad(x):
+    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
+
+
+def loss_and_grad(params, xyz, tri7, labels, T, label_scale, bf=True):
+    """Mean squared error of a batch and its gradient (flat, the library's layout).
+
+    xyz (N, 3) source landmarks; tri7 (B, Et, 7) target features; labels (B, N, 3T)."""
+    r = to_bf16 if bf else (lambda v: np.asarray(v, dtype=np.float64))
+    params = np.asarray(params, dtype=np.float64)
+    L = unpack(params, T)
+    B, Et, _ = tri7.shape
+    N = xyz.shape[0]
+    n_out = 3 * T
+    # target branch
+    xt = np.zeros((B, Et, TRI_IN))
+    xt[:, :, :7] = tri7
+    xt = r(xt)
+    (W1, b1), (W2, b2), (P1, c1), (P2, c2), (P3, c3) = L
+    pre_t = xt @ r(W1).T + b1
+    h1 = r(gelu(pre_t))
+    h2 = h1 @ r(W2).T + b2
+    arg = np.argmax(h2, axis=1)                     # (B, 64): first maximum
+    g = np.take_along_axis(h2, arg[:, None, :], axis=1)[:, 0, :]
+    # point branch
+    xp = np.zeros((B, N, PT_IN))
+    xp[:, :, :3] = xyz[None]
+    xp[:, :, 3:3 + TRI_H] = g[:, None, :]
+    xp = r(xp)
+    pre1 = xp @ r(P1).T + c1
+    a1 = r(gelu(pre1))
+    pre2 = a1 @ r(P2).T + c2
+    a2 = r(gelu(pre2))
+    y = a2 @ r(P3).T + c3
+    count = B * N * n_out
+    e = y[:, :, :n_out] - labels / label_scale
+    loss = float(np.sum(e * e) / count)
+    dy = np.zeros_like(y)
+    dy[:, :, :n_out] = 2.0 * e / count
+    dy = r(dy)
+    grads = []
+    dP3 = np.einsum("bno,bni->oi", dy, a2)
+    dc3 = dy.sum(axis=(0, 1))
+    da2 = r((dy @ r(P3)) * gelu_grad(pre2))
+    dP2 = np.einsum("bno,bni->oi", da2, a1)
+    dc2 = da2.sum(axis=(0, 1))
+    da1 = r((da2 @ r(P2)) * gelu_grad(pre1))
+    dP1 = np.einsum("bno,bni->oi", da1, xp)
+    dc1 = da1.sum(axis=(0, 1))
+    dg = da1.sum(axis=1) @ P1[:, 3:3 + TRI_H]       # FP32 master weights, as on the GPU
+    dh2 = np.zeros((B, Et, TRI_H))
+    bi = np.arange(B)[:, None]
+    ci = np.arange(TRI_H)[None, :]
+    dh2[bi, arg, ci] = dg
+    dh2 = r(dh2)
+    dW2 = np.einsum("bno,bni->oi", dh2, h1)
+    db2 = dh2.sum(axis=(0, 1))
+    dh1 = r((dh2 @ r(W2)) * gelu_grad(pre_t))
+    dW1 = np.einsum("bno,bni->oi", dh1, xt)
+    db1 = dh1.sum(axis=(0, 1))
+    for dW, db in ((dW1, db1), (dW2, db2), (dP1, dc1), (dP2, dc2), (dP3, dc3)):
+        grads += [dW.ravel(), db.ravel()]
+    return loss, np.concatenate(grads)
+
+
+def init_params(T, seed=0):
+    """Random parameters in the library's layout (real entries only, padding zero)."""
+    rng = np.random.default_rng(seed)
+    real = [(7, TRI_H), (TRI_H, TRI_H), (3 + TRI_H, PT_H), (PT_H, PT_H), (PT_H, 3 * T)]
+    out = []
+    for (i, o), (ir, orr) in zip(layer_dims(T), real):
+        W = np.zeros((o, i))
+        W[:orr, :ir] = rng.uniform(-1, 1, size=(orr, ir)) / np.sqrt(ir)
+        b = np.zeros(o)
+        b[:orr] = rng.uniform(-1, 1, size=orr) / np.sqrt(ir)
+        out += [W.ravel(), b]
+    return np.concatenate(out)
+
+
+def predict(params, xyz, tri7, T, label_scale, bf=True):
+    """Predicted momenta, (B, T, N, 3): the library's lddmm_ws_predict in FP64."""
+    r = to_bf16 if bf else (lambda v: np.asarray(v, dtype=np.float64))
+    L = unpack(np.asarray(params, dtype=np.float64), T)
+    B, Et, _ = tri7.shape
+    N = xyz.shape[0]
+    (W1, b1), (W2, b2), (P1, c1), (P2, c2), (P3, c3) = L
+    xt = np.zeros((B, Et, TRI_IN))
+    xt[:, :, :7] = tri7
+    h1 = r(gelu(r(xt) @ r(W1).T + b1))
+    g = (h1 @ r(W2).T + b2).max(axis=1)
+    xp = np.zeros((B, N, PT_IN))
+    xp[:, :, :3] = xyz[None]
+    xp[:, :, 3:3 + TRI_H] = g[:, None, :]
+    a1 = r(gelu(r(xp) @ r(P1).T + c1))
+    a2 = r(gelu(a1 @ r(P2).T + c2))
+    y = (a2 @ r(P3).T + c3)[:, :, :3 * T] * label_scale
+    return y.reshape(B, N, T, 3).transpose(0, 2, 1, 3)

@@ -1,0 +1,104 @@
+"""Warm-start network on the GPU (C ABI lddmm_ws_*): the tensor-core GEMM against an
+FP32 product of the same BF16 operands, the network's loss, gradient and prediction
+against the CPU oracle (oracle/mlp_oracle.py, BF16 rounding at the same points), and
+training reducing the loss."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import mlp_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ws_mod():
+    from lddmm_b200 import warmstart
+
+    return warmstart
+
+
+@pytest.mark.parametrize("m,n,k", [(300, 256, 80), (1000, 32, 256), (64, 16, 16),
+                                   (513, 64, 1024)])
+def test_gemm_bf16_vs_fp32_product(ws_mod, m, n, k):
+    import ctypes as C
+
+    from lddmm_b200 import _lib
+
+    g = torch.Generator(device="cpu").manual_seed(m + n + k)
+    a = torch.randn(m, k, generator=g).to(torch.bfloat16).cuda()
+    b = (0.1 * torch.randn(n, k, generator=g)).to(torch.bfloat16).cuda()
+    c = torch.full((m, n), float("nan"), dtype=torch.float32, device="cuda")
+    _lib.check_ws(_lib.lib.lddmm_ws_gemm_bf16(C.c_void_p(a.data_ptr()), k,
+                                              C.c_void_p(b.data_ptr()), k, m, n, k,
+                                              C.c_void_p(c.data_ptr()), n, None))
+    torch.cuda.synchronize()
+    ref = a.double() @ b.double().T
+    err = (c.double() - ref).abs().max().item() / ref.abs().max().item()
+    assert err < 1e-5, err
+
+
+def _case(T=3, B=3, N=50, Et=40, seed=0):
+    rng = np.random.default_rng(seed)
+    xyz = rng.normal(size=(N, 3))
+    tri7 = rng.normal(size=(B, Et, 7))
+    labels = rng.normal(size=(B, N, 3 * T)) * 0.05
+    return xyz, tri7, labels
+
+
+def _per_layer_rel(g, ref, T):
+    out, off = [], 0
+    for i, o in M.layer_dims(T):
+        for n in (o * i, o):
+            a, b = g[off:off + n], ref[off:off + n]
+            out.append(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)))
+            off += n
+    return out
+
+
+def test_loss_and_gradient_vs_oracle(ws_mod):
+    T, scale = 3, 0.05
+    xyz, tri7, labels = _case(T)
+    params = M.init_params(T, seed=4).astype(np.float32)
+    with ws_mod.WarmStart(xyz, T, batch_max=4, tri_max=64, label_scale=scale) as ws:
+        ws.params = params
+        loss, g = ws.grad(torch.from_numpy(tri7.astype(np.float32)).cuda(),
+                          torch.from_numpy(labels.astype(np.float32)).cuda())
+    lo, go = M.loss_and_grad(params.astype(np.float64), xyz.astype(np.float32).astype(np.float64),
+                             tri7.astype(np.float32).astype(np.float64),
+                             labels.astype(np.float32).astype(np.float64), T, scale, bf=True)
+    assert abs(loss - lo) <= 1e-4 * abs(lo)
+    rels = _per_layer_rel(g.astype(np.float64), go, T)
+    assert max(rels) < 2e-2, rels
+    assert np.linalg.norm(g - go) / np.linalg.norm(go) < 5e-3
+
+
+def test_predict_vs_oracle(ws_mod):
+    T, scale = 3, 0.05
+    xyz, tri7, _ = _case(T, seed=1)
+    params = M.init_params(T, seed=5).astype(np.float32)
+    with ws_mod.WarmStart(xyz, T, batch_max=4, tri_max=64, label_scale=scale) as ws:
+        ws.params = params
+        a = ws.predict(torch.from_numpy(tri7.astype(np.float32)).cuda()).cpu().numpy()
+    ref = M.predict(params.astype(np.float64), xyz.astype(np.float32).astype(np.float64),
+                    tri7.astype(np.float32).astype(np.float64), T, scale, bf=True)
+    ref = ref.reshape(a.shape)
+    assert np.max(np.abs(a - ref)) <= 1e-3 * np.max(np.abs(ref))
+
+
+def test_training_reduces_loss(ws_mod):
+    """Adam steps on a batch whose labels are a smooth function of the landmark
+    positions (learnable from the network's inputs)."""
+    T, scale = 3, 0.05
+    xyz, tri7, _ = _case(T, B=4, seed=2)
+    w = np.random.default_rng(9).normal(size=(3, 3 * T))
+    labels = np.broadcast_to(0.05 * np.sin(xyz @ w), (4, xyz.shape[0], 3 * T)).copy()
+    t = torch.from_numpy(tri7.astype(np.float32)).cuda()
+    y = torch.from_numpy(labels.astype(np.float32)).cuda()
+    with ws_mod.WarmStart(xyz, T, batch_max=4, tri_max=64, label_scale=scale, seed=7) as ws:
+        first = ws.train_step(t, y, 3e-3)
+        for _ in range(200):
+            last = ws.train_step(t, y, 3e-3)
+        p1 = ws.params
+    assert last < 0.2 * first, (first, last)
+    assert np.all(np.isfinite(p1))

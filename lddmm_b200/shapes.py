@@ -12,6 +12,7 @@ lengths) follows ``landmarksToVarifoldKernel`` (``Cpp/src/varifold3D.cpp:8-39``,
 """
 from __future__ import annotations
 
+import functools
 import math
 
 import numpy as np
@@ -44,7 +45,14 @@ def square_boundary(n: int, half: float = 1.0):
 
 def icosphere(subdiv: int, radius: float = 1.0):
     """Icosahedron subdivided ``subdiv`` times, vertices projected to the sphere.
-    10*4^k + 2 vertices, 20*4^k triangles (k = 4: 2562 / 5120)."""
+    10*4^k + 2 vertices, 20*4^k triangles (k = 4: 2562 / 5120).  Returns new arrays
+    (the unit mesh of each subdivision level is built once per process)."""
+    v, f = _unit_icosphere(subdiv)
+    return v * radius, f.copy()
+
+
+@functools.lru_cache(maxsize=None)
+def _unit_icosphere(subdiv: int):
     t = (1.0 + math.sqrt(5.0)) / 2.0
     v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0],
                   [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
@@ -74,9 +82,11 @@ def icosphere(subdiv: int, radius: float = 1.0):
             nf += [[a, ab, ca], [b, bc, ab], [c, ca, bc], [ab, bc, ca]]
         f = np.array(nf, dtype=np.int64)
         verts = vl
-    V = np.array(verts, dtype=np.float64) * radius
-    F = _orient_outward(V, f)
-    return V, F.astype(np.int32)
+    V = np.array(verts, dtype=np.float64)
+    F = _orient_outward(V, f).astype(np.int32)
+    V.setflags(write=False)
+    F.setflags(write=False)
+    return V, F
 
 
 def cube_surface(n: int, half: float = 1.0):

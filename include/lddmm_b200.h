@@ -227,6 +227,14 @@ int lddmm_ctx_counters(const lddmm_ctx *ctx, long long *out, int n);
  * the backward time-loop sweep and the fused optimiser update (-1 when not run). */
 int lddmm_ctx_timeline(const lddmm_ctx *ctx, double *us6);
 
+/* Health check of the bounded device waits (no counterpart in the reference).  Runs
+ * one grid barrier of the kind the persistent sweeps and the L-BFGS cycle use, on two
+ * co-resident CTAs.  never_released = 0: the barrier completes and the call returns 0.
+ * never_released != 0: nothing can complete it; every CTA gives up after about a
+ * second of polling, the kernel ends, and the call returns LDDMM_ERR_TIMEOUT with the
+ * device still usable.  *ms (may be NULL) receives the kernel's duration. */
+int lddmm_wait_selftest(int device, int never_released, double *ms);
+
 /* FP32 FMA throughput of this GPU (TFLOP/s, FMA = 2 flops) measured by a probe
  * kernel of independent FMA chains over every SM; the roofline denominator of the
  * FP32-bound sweeps.  Returns 0 and writes the figure to *tflops. */

@@ -26,7 +26,7 @@ EXPORTS = [
     "lddmm_fp32_peak", "lddmm_multiply_kernel_noalloc", "lddmm_ctx_timeline",
     "lddmm_ws_create", "lddmm_ws_destroy", "lddmm_ws_last_error", "lddmm_ws_num_params",
     "lddmm_ws_params", "lddmm_ws_grad", "lddmm_ws_train_step", "lddmm_ws_predict",
-    "lddmm_ws_gemm_bf16",
+    "lddmm_ws_gemm_bf16", "lddmm_wait_selftest",
 ]
 
 ERRORS = {
@@ -108,6 +108,7 @@ def _load():
     L.lddmm_ctx_counters.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.c_int]
     L.lddmm_fp32_peak.argtypes = [C.c_int, _dp]
     L.lddmm_ctx_timeline.argtypes = [C.c_void_p, _dp]
+    L.lddmm_wait_selftest.argtypes = [C.c_int, C.c_int, _dp]
     L.lddmm_multiply_kernel_noalloc.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                                 C.c_int, C.c_double, C.c_void_p, C.c_void_p]
     # learned warm start

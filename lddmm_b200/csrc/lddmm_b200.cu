@@ -53,6 +53,8 @@ void set_err(const char *fmt, ...) {
 constexpr int kWarps = 4;  // warps per sweep CTA
 // persistent sweeps are chosen automatically up to this many row groups per resident CTA
 constexpr int kPersistAutoUnits = 2;
+// polls of the wait self-test's barrier before it gives up (about a second)
+constexpr unsigned int kSelftestSpin = 1u << 20;
 
 // Device memory of the contexts comes from one stream-ordered pool per device, owned
 // by the library: allocation, zeroing and release are ordered on the context's stream,
@@ -2048,6 +2050,59 @@ extern "C" int lddmm_fp32_peak(int device, double *tflops) {
 }
 
 // ================================================================ misc
+
+// ============================================================ wait self-test
+
+// One grid barrier on a cooperative grid of two CTAs.  With never_released the target
+// is one arrival more than the grid, so nothing can complete it: every CTA must give
+// up after `spin` polls, record the wait in the error word and leave.
+__global__ void wait_selftest_kernel(StepSync *sy, int never_released, unsigned int spin) {
+  const unsigned int target = gridDim.x + (never_released ? 1u : 0u);
+  if (grid_barrier(sy, target, 4242u, spin)) grid_depart(sy);
+}
+
+extern "C" int lddmm_wait_selftest(int device, int never_released, double *ms) {
+  CU(cudaSetDevice(device));
+  cudaStream_t st = nullptr;
+  CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  StepSync *sy = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = dalloc(st, &sy, 1);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e == cudaSuccess) e = cudaEventRecord(e0, st);
+  if (e == cudaSuccess) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2);
+    cfg.blockDim = dim3(32);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    e = cudaLaunchKernelEx(&cfg, wait_selftest_kernel, sy, never_released, kSelftestSpin);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+  unsigned int w[2] = {0, 0};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w, sy, sizeof(w), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  float t = 0.0f;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+  if (sy) cudaFreeAsync(sy, st);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaStreamSynchronize(st);
+  cudaStreamDestroy(st);
+  CU(e);
+  if (ms) *ms = t;
+  if (w[1]) {
+    set_err("wait self-test: the grid barrier gave up (tag %u), as a barrier that nothing "
+            "can complete must", w[1] - 1);
+    return LDDMM_ERR_TIMEOUT;
+  }
+  return 0;
+}
 
 extern "C" const char *lddmm_last_error(void) { return g_err.c_str(); }
 extern "C" const char *lddmm_version(void) { return "lddmm_b200 0.1 (sm_100a)"; }

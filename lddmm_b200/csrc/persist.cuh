@@ -92,7 +92,8 @@ __device__ __forceinline__ unsigned int ld_relaxed(const unsigned int *p) {
 // iteration (the error word is read every 64th); the fence after the loop orders the
 // CTA's later reads after the arrivals it observed.
 __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
-                                             unsigned int tag) {
+                                             unsigned int tag,
+                                             unsigned int spin = kSpinLimit) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -102,7 +103,7 @@ __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
     unsigned int n = 0;
     while (ld_relaxed(&sy->arrive) < target) {
       if ((++n & 63u) == 0u) {
-        if (ld_relaxed(&sy->error) != 0u || n > kSpinLimit) {
+        if (ld_relaxed(&sy->error) != 0u || n > spin) {
           atomicCAS(&sy->error, 0u, 1u + tag);
           ok = 0;
           break;

@@ -192,6 +192,7 @@ struct lddmm_ctx {
   cudaError_t (*adjoint_all)(lddmm_ctx &, double *g) = nullptr;
   int (*pers_blocks)(int which) = nullptr;  // resident CTAs per SM of the persistent kernels
   cudaError_t (*varifold)(lddmm_ctx &) = nullptr;
+  int (*vfd_clusters)(int S) = nullptr;  // co-resident clusters of S varifold CTAs
   cudaError_t (*tt)(lddmm_ctx &, int p, double *part, dim3 grid, double cw, double dw) = nullptr;
 
   ~lddmm_ctx();
@@ -378,7 +379,9 @@ static cudaError_t varifold_impl(lddmm_ctx &c) {
   op.dcdd = c.dcdd;
   op.tile_part = c.vfd_part;
   op.ow2 = c.ow2;
-  return launch_sweep(op, c.el_items, c.n_el_items, c.S_vfd, c.stream);
+  return launch(sweep_packed_kernel<VarifoldOp<D, CT, DT>, kWarps>,
+                (unsigned)(c.n_el_items * c.S_vfd), kWarps * 32, c.S_vfd, c.stream, op,
+                (const int2 *)c.el_items, c.S_vfd);
 }
 
 template <int D, char CT, char DT>
@@ -412,9 +415,29 @@ static bool pick_def(int order, lddmm_ctx &c) {
 }
 
 template <int D, char CT, char DT>
+static int vfd_clusters_impl(int S) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(S * 148));
+  cfg.blockDim = dim3(kWarps * 32);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)S;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int n = 0;
+  const cudaError_t e =
+      cudaOccupancyMaxActiveClusters(&n, sweep_packed_kernel<VarifoldOp<D, CT, DT>, kWarps>, &cfg);
+  cudaGetLastError();
+  return e == cudaSuccess ? n : 0;
+}
+
+template <int D, char CT, char DT>
 static void set_vfd(lddmm_ctx &c) {
   c.varifold = varifold_impl<D, CT, DT>;
   c.tt = tt_impl<D, CT, DT>;
+  c.vfd_clusters = vfd_clusters_impl<D, CT, DT>;
 }
 
 template <int D, char CT>
@@ -967,9 +990,19 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   c.S_shoot = cf.cluster_shoot > 0 ? cf.cluster_shoot : default_cluster(c.n_pt_items);
   c.S_adj = cf.cluster_adjoint > 0 ? cf.cluster_adjoint : default_cluster(c.n_pt_items);
   c.S_vfd = cf.cluster_varifold > 0 ? cf.cluster_varifold : default_cluster(c.n_el_items);
+  if (cf.cluster_varifold <= 0 && c.has_vfd && c.vfd_clusters) {
+    // the largest split whose clusters all fit in one resident wave (clusters are
+    // placed within a GPC, so the count comes from cudaOccupancyMaxActiveClusters; a
+    // partial second wave costs more than the extra split gains: measured 125 us at
+    // S = 5 vs 134-150 us at 6-8 for 80 element tiles)
+    int S = 0;
+    for (int s = 8; s >= 1 && !S; --s)
+      if (c.n_el_items <= c.vfd_clusters(s)) S = s;
+    if (S) c.S_vfd = S;
+  }
   for (int *s : {&c.S_shoot, &c.S_adj, &c.S_vfd})
-    if (*s != 1 && *s != 2 && *s != 4 && *s != 8) {
-      set_err("cluster sizes must be 1, 2, 4 or 8");
+    if (*s < 1 || *s > 8) {
+      set_err("cluster sizes must be 1..8");
       return LDDMM_ERR_ARG;
     }
   // persistent multi-step sweeps: used when one step of the batch does not fill the

@@ -402,6 +402,103 @@ struct VarifoldOp {
       acc[NA - 1] = fmaf(-ang, td, acc[NA - 1] + tb);
     }
   }
+  // ---- packed form (sweep_packed_kernel): a lane's two rows in one FP32x2 operation.
+  // Staged j point: the values -ch, -cl, n, w each stored twice:
+  //   3D: (-chx,-chx,-chy,-chy) (-chz,-chz,-clx,-clx) (-cly,-cly,-clz,-clz)
+  //       (nx,nx,ny,ny) (nz,nz,w,w)
+  //   2D: (-chx,-chx,-chy,-chy) (-clx,-clx,-cly,-cly) (nx,nx,ny,ny) (w,w,-,-)
+  static constexpr bool kPacked = true;
+  static constexpr int JWP = (D == 3) ? 5 : 4;
+  struct IData2 {
+    float2 ch[D], cl[D], n[D];  // (row0, row1)
+  };
+  __device__ void load_i2(int p, int r0, int r1, IData2 &I) const {
+    IData a, b;
+    load_i(p, r0, a);
+    load_i(p, r1, b);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      I.ch[d] = make_float2(a.ch[d], b.ch[d]);
+      I.cl[d] = make_float2(a.cl[d], b.cl[d]);
+      I.n[d] = make_float2(a.n[d], b.n[d]);
+    }
+  }
+  __device__ void load_j2(int p, int j, float4 (&w)[JWP]) const {
+    float4 v[JW];
+    load_j(p, j, v);
+    if (D == 3) {
+      // v: (chx chy chz wt) (nx ny nz clx) (cly clz - -)
+      w[0] = make_float4(-v[0].x, -v[0].x, -v[0].y, -v[0].y);
+      w[1] = make_float4(-v[0].z, -v[0].z, -v[1].w, -v[1].w);
+      w[2] = make_float4(-v[JW - 1].x, -v[JW - 1].x, -v[JW - 1].y, -v[JW - 1].y);
+      w[3] = make_float4(v[1].x, v[1].x, v[1].y, v[1].y);
+      w[JWP - 1] = make_float4(v[1].z, v[1].z, v[0].w, v[0].w);
+    } else {
+      // v: (chx chy clx cly) (nx ny wt -)
+      w[0] = make_float4(-v[0].x, -v[0].x, -v[0].y, -v[0].y);
+      w[1] = make_float4(-v[0].z, -v[0].z, -v[0].w, -v[0].w);
+      w[2] = make_float4(v[1].x, v[1].x, v[1].y, v[1].y);
+      w[JWP - 1] = make_float4(v[1].z, v[1].z, 0.0f, 0.0f);
+    }
+  }
+  template <int SET>
+  __device__ __forceinline__ void pair2(const IData2 &I, const float4 (&w)[JWP],
+                                        float2 (&acc)[NA]) const {
+    float2 mch[D], mcl[D], nj[D], wt;
+    if (D == 3) {
+      mch[0] = make_float2(w[0].x, w[0].y); mch[1] = make_float2(w[0].z, w[0].w);
+      mch[D - 1] = make_float2(w[1].x, w[1].y);
+      mcl[0] = make_float2(w[1].z, w[1].w); mcl[1] = make_float2(w[2].x, w[2].y);
+      mcl[D - 1] = make_float2(w[2].z, w[2].w);
+      nj[0] = make_float2(w[3].x, w[3].y); nj[1] = make_float2(w[3].z, w[3].w);
+      nj[D - 1] = make_float2(w[JWP - 1].x, w[JWP - 1].y);
+      wt = make_float2(w[JWP - 1].z, w[JWP - 1].w);
+    } else {
+      mch[0] = make_float2(w[0].x, w[0].y); mch[1] = make_float2(w[0].z, w[0].w);
+      mcl[0] = make_float2(w[1].x, w[1].y); mcl[1] = make_float2(w[1].z, w[1].w);
+      nj[0] = make_float2(w[2].x, w[2].y); nj[1] = make_float2(w[2].z, w[2].w);
+      wt = make_float2(w[JWP - 1].x, w[JWP - 1].y);
+    }
+    // the scalar pair() computes nr2 = sum fma(-dc, dc, .) = -r2 exactly
+    float2 dc[D], r2 = make_float2(0.0f, 0.0f), ang = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      dc[d] = __fadd2_rn(__fadd2_rn(I.ch[d], mch[d]), __fadd2_rn(I.cl[d], mcl[d]));
+      r2 = __ffma2_rn(dc[d], dc[d], r2);
+      ang = __ffma2_rn(I.n[d], nj[d], ang);
+    }
+    float kx, ky, gx, gy;
+    CenKernel<CT>::val_w(-r2.x, kx, gx);
+    CenKernel<CT>::val_w(-r2.y, ky, gy);
+    const float2 k = make_float2(kx, ky);
+    const float2 kw = __fmul2_rn(k, wt);
+    if (kBinet) {
+      const float2 t1 = __fmul2_rn(kw, ang);  // k w b'/2
+      const float2 tb = __fmul2_rn(t1, ang);  // k w b
+      acc[SET] = __fadd2_rn(acc[SET], tb);
+      const float2 cg_ = (CT == 'G') ? tb : __fmul2_rn(tb, k);  // kg w b
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        acc[2 + d] = __ffma2_rn(t1, nj[d], acc[2 + d]);
+        acc[2 + D + d] = __ffma2_rn(cg_, dc[d], acc[2 + D + d]);
+      }
+    } else {
+      float bx, dbx, by, dby;
+      DirKernel<DT>::val_d(ang.x, ow2, bx, dbx);
+      DirKernel<DT>::val_d(ang.y, ow2, by, dby);
+      const float2 tb = __fmul2_rn(kw, make_float2(bx, by));
+      const float2 td = __fmul2_rn(kw, make_float2(dbx, dby));
+      acc[SET] = __fadd2_rn(acc[SET], tb);
+      const float2 cg_ = (CT == 'G') ? tb : __fmul2_rn(tb, k);
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        acc[2 + d] = __ffma2_rn(td, nj[d], acc[2 + d]);
+        acc[2 + D + d] = __ffma2_rn(cg_, dc[d], acc[2 + D + d]);
+      }
+      acc[NA - 1] = __ffma2_rn(make_float2(-ang.x, -ang.y), td,
+                               __fadd2_rn(acc[NA - 1], tb));
+    }
+  }
   __device__ double finalize(int p, int row, const double (&v)[NA]) const {
     const PairDesc &P = pd[p];
     if (row >= P.Ed) return 0.0;

@@ -29,6 +29,16 @@
 //   finalize(p, row, acc)       consume the full FP64 row sums; returns a value
 //                               that is summed over the tile
 //   write_tile(p, tile, v)      store the tile sum
+//
+// sweep_packed_kernel is the same sweep for Ops that also evaluate a lane's two rows
+// at once in packed FP32x2 arithmetic (sm_100 FFMA2 / FADD2 / FMUL2: one instruction,
+// two independent IEEE operations), given
+//   JWP, IData2        float4 words of a staged j point whose values are stored twice,
+//                      (v, v), so both halves of a packed operand come from one
+//                      shared-memory load; the two rows' registers, (row0, row1)
+//   load_i2(p, r0, r1, I), load_j2(p, j, w), pair2<SET>(I, w, acc)  with float2 acc
+// Each packed operation applies to each row exactly the scalar operation of pair()
+// in the same order, so both kernels give bitwise the same sums.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -57,15 +67,124 @@ __device__ __forceinline__ void run_sub(const Op &op, const float4 (*sj)[kSub], 
   }
 }
 
+// Warps -> CTA (shared memory) -> cluster (DSMEM) reduction of a tile's row sums and
+// the finalisation by cluster rank 0 (shared by both sweep kernels).
+template <class Op, int W>
+__device__ __forceinline__ void finish_tile(const Op &op, int p, int tile, int rank, int S,
+                                            const float (&hi0)[Op::NA], const float (&lo0)[Op::NA],
+                                            const float (&hi1)[Op::NA], const float (&lo1)[Op::NA]) {
+  constexpr int NA = Op::NA;
+  __shared__ double s_red[W][kTile][NA];
+  __shared__ double s_cta[kTile][NA];
+  __shared__ double s_scr[W];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int a = 0; a < NA; ++a) {
+    s_red[warp][lane][a] = (double)hi0[a] + (double)lo0[a];
+    s_red[warp][32 + lane][a] = (double)hi1[a] + (double)lo1[a];
+  }
+  __syncthreads();
+  double v[NA];
+  if (threadIdx.x < kTile) {
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+      double s = 0.0;
+      for (int w = 0; w < W; ++w) s += s_red[w][threadIdx.x][a];
+      v[a] = s;
+      s_cta[threadIdx.x][a] = s;
+    }
+  }
+  if (S > 1) {
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    if (rank == 0 && threadIdx.x < kTile) {
+      for (int r = 1; r < S; ++r) {
+        const double *rem = cluster.map_shared_rank(&s_cta[0][0], r);
+#pragma unroll
+        for (int a = 0; a < NA; ++a) v[a] += rem[threadIdx.x * NA + a];
+      }
+    }
+    cluster.sync();
+  }
+  if (rank != 0) return;
+  double e = 0.0;
+  if (threadIdx.x < kTile) e = op.finalize(p, tile * kTile + threadIdx.x, v);
+  if (Op::kTileSum) {
+    const double tot = block_sum(e, s_scr);
+    if (threadIdx.x == 0) op.write_tile(p, tile, tot);
+  }
+}
+
+template <int SET, class Op>
+__device__ __forceinline__ void run_sub2(const Op &op, const float4 (*sj)[kSub], int lo, int hi,
+                                         const typename Op::IData2 &I, float2 (&a)[Op::NA]) {
+#pragma unroll 8
+  for (int jj = lo; jj < hi; ++jj) {
+    float4 w[Op::JWP];
+#pragma unroll
+    for (int x = 0; x < Op::JWP; ++x) w[x] = sj[x][jj];
+    op.template pair2<SET>(I, w, a);
+  }
+}
+
+template <class Op, int W>
+__global__ void __launch_bounds__(W * 32)
+    sweep_packed_kernel(const Op op, const int2 *__restrict__ items, int S) {
+  constexpr int JWP = Op::JWP;
+  constexpr int NA = Op::NA;
+  __shared__ float4 s_j[W][JWP][kSub];
+  const int item = blockIdx.x / S;
+  const int rank = blockIdx.x - item * S;
+  const int2 it = items[item];  // static work list
+  pdl_wait();
+  pdl_trigger();
+  const int p = it.x, tile = it.y;
+  if (!op.active(p)) return;  // identical for every CTA of the cluster
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  typename Op::IData2 I;
+  op.load_i2(p, tile * kTile + lane, tile * kTile + 32 + lane, I);
+  float hi0[NA], lo0[NA], hi1[NA], lo1[NA];
+#pragma unroll
+  for (int a = 0; a < NA; ++a) hi0[a] = lo0[a] = hi1[a] = lo1[a] = 0.0f;
+  const int J = op.j_count(p);
+  const int nw = S * W, gw = rank * W + warp;
+  const int jb = (int)((long long)J * gw / nw), je = (int)((long long)J * (gw + 1) / nw);
+  const int split = Op::kTwoSets ? op.set_boundary(p) : J;
+  float4 nxt[JWP];
+  if (jb + lane < je) op.load_j2(p, jb + lane, nxt);
+  for (int j0 = jb; j0 < je; j0 += kSub) {
+    __syncwarp();
+#pragma unroll
+    for (int x = 0; x < JWP; ++x) s_j[warp][x][lane] = nxt[x];
+    __syncwarp();
+    const int cnt = min(kSub, je - j0);
+    const int jn = j0 + kSub;
+    if (jn + lane < je) op.load_j2(p, jn + lane, nxt);
+    float2 a[NA];
+#pragma unroll
+    for (int k = 0; k < NA; ++k) a[k] = make_float2(0.0f, 0.0f);
+    if (Op::kTwoSets) {
+      const int b = min(max(split - j0, 0), cnt);  // [0, b) first set, [b, cnt) second
+      if (b > 0) run_sub2<0>(op, s_j[warp], 0, b, I, a);
+      if (b < cnt) run_sub2<1>(op, s_j[warp], b, cnt, I, a);
+    } else {
+      run_sub2<0>(op, s_j[warp], 0, cnt, I, a);
+    }
+#pragma unroll
+    for (int k = 0; k < NA; ++k) {
+      two_sum_acc(hi0[k], lo0[k], a[k].x);
+      two_sum_acc(hi1[k], lo1[k], a[k].y);
+    }
+  }
+  finish_tile<Op, W>(op, p, tile, rank, S, hi0, lo0, hi1, lo1);
+}
+
 template <class Op, int W>
 __global__ void __launch_bounds__(W * 32) sweep_kernel(const Op op, const int2 *__restrict__ items,
                                                        int S) {
   constexpr int JW = Op::JW;
   constexpr int NA = Op::NA;
   __shared__ float4 s_j[W][JW][kSub];
-  __shared__ double s_red[W][kTile][NA];
-  __shared__ double s_cta[kTile][NA];
-  __shared__ double s_scr[W];
 
   const int item = blockIdx.x / S;
   const int rank = blockIdx.x - item * S;
@@ -116,41 +235,7 @@ __global__ void __launch_bounds__(W * 32) sweep_kernel(const Op op, const int2 *
     }
   }
 
-#pragma unroll
-  for (int a = 0; a < NA; ++a) {
-    s_red[warp][lane][a] = (double)hi0[a] + (double)lo0[a];
-    s_red[warp][32 + lane][a] = (double)hi1[a] + (double)lo1[a];
-  }
-  __syncthreads();
-  double v[NA];
-  if (threadIdx.x < kTile) {
-#pragma unroll
-    for (int a = 0; a < NA; ++a) {
-      double s = 0.0;
-      for (int w = 0; w < W; ++w) s += s_red[w][threadIdx.x][a];
-      v[a] = s;
-      s_cta[threadIdx.x][a] = s;
-    }
-  }
-  if (S > 1) {
-    cg::cluster_group cluster = cg::this_cluster();
-    cluster.sync();
-    if (rank == 0 && threadIdx.x < kTile) {
-      for (int r = 1; r < S; ++r) {
-        const double *rem = cluster.map_shared_rank(&s_cta[0][0], r);
-#pragma unroll
-        for (int a = 0; a < NA; ++a) v[a] += rem[threadIdx.x * NA + a];
-      }
-    }
-    cluster.sync();
-  }
-  if (rank != 0) return;
-  double e = 0.0;
-  if (threadIdx.x < kTile) e = op.finalize(p, tile * kTile + threadIdx.x, v);
-  if (Op::kTileSum) {
-    const double tot = block_sum(e, s_scr);
-    if (threadIdx.x == 0) op.write_tile(p, tile, tot);
-  }
+  finish_tile<Op, W>(op, p, tile, rank, S, hi0, lo0, hi1, lo1);
 }
 
 }  // namespace lddmm

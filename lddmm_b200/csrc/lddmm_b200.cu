@@ -471,7 +471,7 @@ static cudaError_t launch_geometry(lddmm_ctx &c, const double *q64T) {
 
 static cudaError_t launch_gather(lddmm_ctx &c, const double *q64T, float4 *un, float4 *ln,
                                  double *dq_out) {
-  const unsigned nb = (unsigned)((c.NPtot + 127) / 128);
+  const unsigned nb = (unsigned)(((long long)c.NPtot * kGatherLanes + 127) / 128);
   if (c.D == 3)
     return launch(gather_kernel<3>, nb, 128, 0, c.stream, c.pd, c.act, c.pt_pair, c.NPtot,
                   c.adj_ptr, c.adj, c.dcdd, q64T, c.XT, c.p64, un, ln, dq_out, c.T);
@@ -481,7 +481,7 @@ static cudaError_t launch_gather(lddmm_ctx &c, const double *q64T, float4 *un, f
 
 static cudaError_t launch_objective(lddmm_ctx &c, PairState *st, double *f_out) {
   const int groups = c.persistent ? kGroup : 0;
-  return launch(objective_kernel, (unsigned)c.P, 128, 0, c.stream, c.pd, c.act, c.reg_part,
+  return launch(objective_kernel, (unsigned)c.P, 512, 0, c.stream, c.pd, c.act, c.reg_part,
                 groups ? c.ngrp_tot : c.ntile_tot, c.vfd_part, c.T, st, f_out, groups);
 }
 

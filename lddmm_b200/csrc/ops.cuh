@@ -14,6 +14,8 @@
 
 namespace lddmm {
 
+constexpr int kGatherLanes = 8;  // lanes per vertex in gather_kernel
+
 // ------------------------------------------------------------------- forward
 
 template <int D, int ORDER>
@@ -600,31 +602,44 @@ __global__ void gather_kernel(const PairDesc *__restrict__ pd, const int *__rest
                               float4 *ls_n, double *dq_out, int T) {
   pdl_wait();
   pdl_trigger();
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= n_pt) return;
-  const int p = pt_pair[g];
-  if (p < 0 || !act[p]) return;
-  const PairDesc &P = pd[p];
-  const int row = g - P.pt_off;
+  // kGatherLanes lanes per vertex, each over every kGatherLanes-th adjacent element, so
+  // the element loads of a vertex are in flight together; the lanes' sums are then
+  // combined by a fixed shuffle tree (deterministic)
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) / kGatherLanes;
+  const int sub = threadIdx.x % kGatherLanes;
+  int p = -1;
+  if (g < n_pt) p = pt_pair[g];
+  const bool live = p >= 0 && act[p];
   double acc[3] = {0.0, 0.0, 0.0};
-  for (int k = adj_ptr[g]; k < adj_ptr[g + 1]; ++k) {
-    const int4 e = adj[k];
-    const double *o = dcdd + (size_t)e.x * (2 * D);
-    if (D == 3) {
-      const double *qa = q64T + (size_t)e.y * 3, *qb = q64T + (size_t)e.z * 3;
-      const double ab[3] = {qa[0] - qb[0], qa[1] - qb[1], qa[2] - qb[2]};
-      const double *dd = o + 3;
-      const double x0 = dd[1] * ab[2] - dd[2] * ab[1];
-      const double x1 = -dd[0] * ab[2] + dd[2] * ab[0];
-      const double x2 = dd[0] * ab[1] - dd[1] * ab[0];
-      acc[0] += o[0] / 3.0 + x0;
-      acc[1] += o[1] / 3.0 + x1;
-      acc[2] += o[2] / 3.0 + x2;
-    } else {
-      acc[0] += 0.5 * o[0] + e.y * o[2];
-      acc[1] += 0.5 * o[1] + e.y * o[3];
+  if (live) {
+    const int k1 = adj_ptr[g + 1];
+    for (int k = adj_ptr[g] + sub; k < k1; k += kGatherLanes) {
+      const int4 e = adj[k];
+      const double *o = dcdd + (size_t)e.x * (2 * D);
+      if (D == 3) {
+        const double *qa = q64T + (size_t)e.y * 3, *qb = q64T + (size_t)e.z * 3;
+        const double ab[3] = {qa[0] - qb[0], qa[1] - qb[1], qa[2] - qb[2]};
+        const double *dd = o + 3;
+        const double x0 = dd[1] * ab[2] - dd[2] * ab[1];
+        const double x1 = -dd[0] * ab[2] + dd[2] * ab[0];
+        const double x2 = dd[0] * ab[1] - dd[1] * ab[0];
+        acc[0] += o[0] / 3.0 + x0;
+        acc[1] += o[1] / 3.0 + x1;
+        acc[2] += o[2] / 3.0 + x2;
+      } else {
+        acc[0] += 0.5 * o[0] + e.y * o[2];
+        acc[1] += 0.5 * o[1] + e.y * o[3];
+      }
     }
   }
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int off = kGatherLanes / 2; off > 0; off >>= 1)
+      acc[d] += __shfl_xor_sync(0xffffffffu, acc[d], off);
+  if (!live || sub != 0) return;
+  const PairDesc &P = pd[p];
+  const int row = g - P.pt_off;
   double pn[3] = {0.0, 0.0, 0.0};
   for (int d = 0; d < D; ++d) {
     if (dq_out) dq_out[(size_t)g * D + d] = acc[d];

@@ -63,8 +63,6 @@ struct PairState {
   double slp, dlen;      // g.d and |d| of the current direction
   double H0;             // initial inverse Hessian scale s.y / y.y
   double stp;            // last accepted step length (t * |d|)
-  double rho[kMaxMem];   // 1 / (s.y) per history slot
-  double alf[kMaxMem];   // two-loop alpha per history slot
   int bisMax, epdMax, bisCnt, epdCnt, objCnt;
   int newIdx, hisNum, itr;
   int phase, status, action, need_dir;

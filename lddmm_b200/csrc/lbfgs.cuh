@@ -1,24 +1,36 @@
 // Device-resident FP64 L-BFGS with the weak-Wolfe line search, for a batch of
 // independent pairs, without host round trips inside an iteration.
 //
-// Semantics: Cpp/src/LBFGS.cpp:25-112 (outer loop, H0 = s.y / y.y, ring buffer,
-// stop at |g| < tol), Cpp/src/getDirection.cpp:9-66 (two-loop recursion),
-// Cpp/src/lineSearch.cpp:26-110 (bracketing by doubling / bisection with the
+// Semantics: Cpp/src/LBFGS.cpp:25-112 (outer loop, H0 = s.y / y.y of the newest pair,
+// ring buffer of memNum pairs, stop at |g| < tol), Cpp/src/getDirection.cpp:9-66 (the
+// direction d = -H g of the limited-memory BFGS matrix H built from those pairs and
+// H0), Cpp/src/lineSearch.cpp:26-110 (bracketing by doubling / bisection with the
 // heuristic limits bisMax = max(50, log2(1e5 |d|)), epdMax = max(10, log2(1e5/|d|))).
 //
-// Execution: every objective evaluation of the batch is followed by one "cycle" of
-// fixed kernels (captured once in a CUDA graph):
+// The direction uses the compact representation of the same matrix (Byrd, Nocedal and
+// Schnabel, "Representations of quasi-Newton matrices and their use in limited memory
+// methods", Math. Programming 63, 1994): with the pairs in chronological order,
+// R = upper triangle of S^T Y, D = its diagonal and gamma = H0,
+//   u = R^-1 (S^T g),   w = R^-T ((D + gamma Y^T Y) u - gamma Y^T g),
+//   H g = gamma g + S w - gamma Y u.
+// In exact arithmetic this is the reference's two-loop recursion; it needs all its dot
+// products in one pass over the vectors instead of 2 m dependent ones.  S^T Y and
+// Y^T Y are kept per pair (slot-indexed) and updated with the newest pair only.
+//
+// Execution: every objective evaluation of the batch is followed by one "cycle":
 //   POST   dots g_t.g_t, g_t.d over the trial gradients
 //   DECIDE per-pair state machine: Wolfe tests, accept / expand / bisect / fail
-//   ACCEPT s = x_t - x, y = g_t - g into the ring, x = x_t, g = g_t; dots s.y, y.y, s.g
-//   B_0..B_{m-1}  first loop of the two-loop recursion (one dot + one axpy per pass)
-//   F_0..F_{m-1}  second loop, right-aligned so every pair ends in F_{m-1}
-//   FIN    d = -r, x_t = x + t d, FP32 copy of x_t for the sweeps; dots g.d, d.d
+//   ACCEPT s = x_t - x, y = g_t - g into the ring, x = x_t, g = g_t; for every history
+//          slot i the dots s_i.y, y_i.y, s_i.g, y_i.g (with the new y and g)
+//   SOLVE  per pair: S^T Y and Y^T Y updated, the small triangular solves -> the
+//          coefficients of g, S and Y in d
+//   FIN    d = -(gamma g + S w - gamma Y u), x_t = x + t d, FP32 copy of x_t for the
+//          sweeps; dots g.d, d.d
 //   LSINIT descent test and line-search limits for pairs with a new direction
-// Each vector pass covers all pairs' variables in chunks of kChunk; a chunk belongs
-// to one pair and writes its partial dots, and the next pass reduces its pair's
-// partials in chunk order (deterministic).  Pairs that do not take part in a pass
-// leave in the first instructions of each CTA.
+// Each vector pass covers all pairs' variables in chunks of kChunk; a chunk belongs to
+// one pair and writes its partial dots, which the next phase reduces in chunk order
+// (deterministic).  Pairs that do not take part in a pass leave in the first
+// instructions of each CTA.
 #pragma once
 
 #include <cfloat>
@@ -31,30 +43,26 @@ namespace lddmm {
 
 constexpr int kChunk = 2048;  // doubles per vector-pass CTA
 constexpr int kVecThreads = 256;
+constexpr int kPartStride = 4 * kMaxMem;  // dot partials per chunk (ACCEPT: 4 per slot)
+constexpr int kDotGroup = 4;              // history slots per accumulation sweep of a chunk
+constexpr int kCoefStride = 1 + 2 * kMaxMem;  // per pair: gamma, S coefficients, Y coefficients
 
-enum PassMode : int { kPost = 0, kAccept = 1, kTwoLoopB = 2, kTwoLoopF = 3, kFin = 4 };
+enum PassMode : int { kPost = 0, kAccept = 1, kFin = 2 };
 
 struct VecArgs {
   const PairDesc *pd;
   PairState *st;
   const int *chunk_pair;
-  double *X, *G, *XT, *GT, *Dv, *Qv, *S, *Y;
+  double *X, *G, *XT, *GT, *Dv, *S, *Y;
   long long nvar;   // stride between ring slots
   float4 *as;       // FP32 trial alpha in point layout [T][NPtot]
   int NPtot;
   int D;
   int m;            // memory
-  const double *part_in;
-  double *part_out;
+  double *part;     // dot partials [chunk][kPartStride]
+  double *SY, *YY;  // per pair [m][m], slot-indexed: SY[i][j] = s_i.y_j (i no newer than j)
+  double *coef;     // per pair [kCoefStride]
 };
-
-// Sum of a pair's chunk partials (component j), by warp 0, fixed order.
-__device__ __forceinline__ double pair_partial(const double *part, int c0, int nc, int j) {
-  double s = 0.0;
-  const int lane = threadIdx.x & 31;
-  for (int c = lane; c < nc; c += 32) s += part[(size_t)(c0 + c) * 3 + j];
-  return warp_sum(s);
-}
 
 __device__ __forceinline__ void store_trial_f32(const VecArgs &A, const PairDesc &P,
                                                 long long v, double x) {
@@ -66,192 +74,212 @@ __device__ __forceinline__ void store_trial_f32(const VecArgs &A, const PairDesc
   f[((size_t)t * A.NPtot + P.pt_off + i) * 4 + d] = (float)x;
 }
 
-// One vector pass over chunk c.  `k` = two-loop pass index for kTwoLoopB / kTwoLoopF.
-// Called by a whole CTA (it synchronises the CTA).
-__device__ void vec_pass_chunk(const VecArgs &A, int mode, int k, int c) {
-  __shared__ double s_scal[4];
-  __shared__ double s_scr[kVecThreads / 32];
+// Block sums of K values per thread (fixed order), written to out[0..K) by threads < K.
+template <int K>
+__device__ __forceinline__ void block_sums(double (&v)[K], double *out, int n_out) {
+  __shared__ double s_red[kVecThreads / 32][K];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) s_red[warp][k] = v[k];
+  __syncthreads();
+  if (threadIdx.x < n_out) {
+    double t = 0.0;
+    for (int w = 0; w < kVecThreads / 32; ++w) t += s_red[w][threadIdx.x];
+    out[threadIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+// Number of valid ring slots: slots 0..h-1 until the ring is full, then all m.
+__device__ __forceinline__ bool slot_valid(int i, int h, int m) { return h >= m || i < h; }
+
+// One vector pass over chunk c.  Called by a whole CTA (it synchronises the CTA).
+__device__ void vec_pass_chunk(const VecArgs &A, int mode, int c) {
+  __shared__ double s_coef[kCoefStride];
   const int p = A.chunk_pair[c];
   const PairDesc &P = A.pd[p];
-  PairState &S = A.st[p];
+  const PairState &S = A.st[p];
   const int m = A.m;
-  const int first = (c == P.chunk_off);
-
-  // ----- participation and scalar set-up (uniform per CTA)
-  bool go = false;
-  int idx = 0, idx_next = -1;  // history slots
-  double coef = 0.0;
-  int final_b = 0;
-  if (mode == kPost) {
+  bool go;
+  if (mode == kPost)
     go = (S.phase == kPhaseInit || S.phase == kPhaseLS) && S.active;
-  } else if (mode == kAccept) {
+  else if (mode == kAccept)
     go = (S.action == kActAccept || S.action == kActAcceptInit);
-  } else if (mode == kTwoLoopB) {
-    go = S.need_dir && k < S.hisNum;
-    if (go) {
-      idx = S.newIdx - k;
-      if (idx < 0) idx += m;
-      double dprev = 0.0, H0 = 0.0, rho = 0.0;
-      if (threadIdx.x < 32) {
-        dprev = pair_partial(A.part_in, P.chunk_off, P.nchunk, k == 0 ? 2 : 0);
-        if (k == 0) {
-          const double sy = pair_partial(A.part_in, P.chunk_off, P.nchunk, 0);
-          const double yy = pair_partial(A.part_in, P.chunk_off, P.nchunk, 1);
-          rho = 1.0 / sy;
-          H0 = sy / yy;
-        }
-      }
-      if (threadIdx.x == 0) {
-        if (k == 0) {
-          s_scal[1] = H0;
-          s_scal[2] = rho;
-        } else {
-          s_scal[1] = S.H0;
-          s_scal[2] = S.rho[idx];
-        }
-        s_scal[0] = s_scal[2] * dprev;  // alpha_idx = rho (s.q)
-      }
-      __syncthreads();
-      coef = s_scal[0];
-      if (first && threadIdx.x == 0) {
-        if (k == 0) {
-          S.H0 = s_scal[1];
-          S.rho[idx] = s_scal[2];
-        }
-        S.alf[idx] = coef;
-      }
-      final_b = (k + 1 == S.hisNum);
-      if (!final_b) {
-        idx_next = idx - 1;
-        if (idx_next < 0) idx_next += m;
-      } else {
-        idx_next = (S.hisNum < m) ? 0 : S.newIdx + 1;  // oldest slot
-        if (idx_next >= m) idx_next -= m;
-      }
-    }
-  } else if (mode == kTwoLoopF) {
-    const int h = k - (m - S.hisNum);
-    go = S.need_dir && h >= 0;
-    if (go) {
-      int old = (S.hisNum < m) ? 0 : S.newIdx + 1;
-      if (old >= m) old -= m;
-      idx = old + h;
-      if (idx >= m) idx -= m;
-      double dprev = 0.0;
-      if (threadIdx.x < 32) dprev = pair_partial(A.part_in, P.chunk_off, P.nchunk, 0);
-      if (threadIdx.x == 0) s_scal[0] = S.alf[idx] - S.rho[idx] * dprev;  // alpha - beta
-      __syncthreads();
-      coef = s_scal[0];
-      if (h + 1 < S.hisNum) {
-        idx_next = idx + 1;
-        if (idx_next >= m) idx_next -= m;
-      }
-    }
-  } else {  // kFin
+  else
     go = S.need_dir || (S.phase == kPhaseLS && S.action == kActNone && S.active);
-  }
   if (!go) return;
 
-  // ----- elementwise work + up to three dots
   const long long base = P.var_off;
   const long long n = P.var_num;
   const long long lo = (long long)(c - P.chunk_off) * kChunk;
   const long long hi = min(lo + kChunk, n);
   const long long NV = A.nvar;
-  double d0 = 0.0, d1 = 0.0, d2 = 0.0;
+  double *out = A.part + (size_t)c * kPartStride;
 
   if (mode == kPost) {
-    for (long long v = lo + threadIdx.x; v < hi; v += kVecThreads) {
-      const double g = A.GT[base + v];
-      d0 += g * g;
-      d1 += g * A.Dv[base + v];
+    double v[2] = {0.0, 0.0};
+    for (long long k = lo + threadIdx.x; k < hi; k += kVecThreads) {
+      const double g = A.GT[base + k];
+      v[0] += g * g;
+      v[1] += g * A.Dv[base + k];
     }
-  } else if (mode == kAccept) {
+    block_sums<2>(v, out, 2);
+    return;
+  }
+  if (mode == kAccept) {
     if (S.action == kActAcceptInit) {
-      for (long long v = lo + threadIdx.x; v < hi; v += kVecThreads) {
-        A.X[base + v] = A.XT[base + v];
-        A.G[base + v] = A.GT[base + v];
+      for (long long k = lo + threadIdx.x; k < hi; k += kVecThreads) {
+        A.X[base + k] = A.XT[base + k];
+        A.G[base + k] = A.GT[base + k];
       }
-    } else {
-      double *Sv = A.S + (size_t)S.newIdx * NV + base;
-      double *Yv = A.Y + (size_t)S.newIdx * NV + base;
-      for (long long v = lo + threadIdx.x; v < hi; v += kVecThreads) {
-        const double xt = A.XT[base + v], gt = A.GT[base + v];
-        const double s = xt - A.X[base + v];
-        const double y = gt - A.G[base + v];
-        Sv[v] = s;
-        Yv[v] = y;
-        A.X[base + v] = xt;
-        A.G[base + v] = gt;
-        d0 += s * y;
-        d1 += y * y;
-        d2 += s * gt;
-      }
+      return;
     }
-  } else if (mode == kTwoLoopB) {
-    const double *Yv = A.Y + (size_t)idx * NV + base;
-    const double *src = (k == 0) ? (A.G + base) : (A.Qv + base);
-    const double H0 = s_scal[1];
-    const double *Nx = final_b ? (A.Y + (size_t)idx_next * NV + base)
-                               : (A.S + (size_t)idx_next * NV + base);
-    for (long long v = lo + threadIdx.x; v < hi; v += kVecThreads) {
-      double q = src[v] - coef * Yv[v];
-      if (final_b) q *= H0;  // r = H0 q
-      A.Qv[base + v] = q;
-      d0 += Nx[v] * q;
+    const int nw = S.newIdx, h = S.hisNum;
+    double *Sn = A.S + (size_t)nw * NV + base;
+    double *Yn = A.Y + (size_t)nw * NV + base;
+    for (long long k = lo + threadIdx.x; k < hi; k += kVecThreads) {
+      const double xt = A.XT[base + k], gt = A.GT[base + k];
+      Sn[k] = xt - A.X[base + k];
+      Yn[k] = gt - A.G[base + k];
+      A.X[base + k] = xt;
+      A.G[base + k] = gt;
     }
-  } else if (mode == kTwoLoopF) {
-    const double *Sv = A.S + (size_t)idx * NV + base;
-    const double *Ny = (idx_next >= 0) ? (A.Y + (size_t)idx_next * NV + base) : nullptr;
-    for (long long v = lo + threadIdx.x; v < hi; v += kVecThreads) {
-      const double r = A.Qv[base + v] + coef * Sv[v];
-      A.Qv[base + v] = r;
-      if (Ny) d0 += Ny[v] * r;
+    // the slot dots with the new y and g, kDotGroup slots per sweep of the chunk (a
+    // thread re-reads only the elements it wrote above)
+    for (int i0 = 0; i0 < m; i0 += kDotGroup) {
+      double v[4 * kDotGroup];
+#pragma unroll
+      for (int q = 0; q < 4 * kDotGroup; ++q) v[q] = 0.0;
+      for (long long k = lo + threadIdx.x; k < hi; k += kVecThreads) {
+        const double y = Yn[k], g = A.G[base + k];
+#pragma unroll
+        for (int q = 0; q < kDotGroup; ++q) {
+          const int i = i0 + q;
+          if (i < m && slot_valid(i, h, m)) {
+            const double si = A.S[(size_t)i * NV + base + k], yi = A.Y[(size_t)i * NV + base + k];
+            v[4 * q + 0] += si * y;
+            v[4 * q + 1] += yi * y;
+            v[4 * q + 2] += si * g;
+            v[4 * q + 3] += yi * g;
+          }
+        }
+      }
+      block_sums<4 * kDotGroup>(v, out + 4 * i0, min(4 * kDotGroup, 4 * (m - i0)));
     }
-  } else {  // kFin
-    if (S.need_dir) {
-      const double *src = (S.hisNum == 0) ? (A.G + base) : (A.Qv + base);
-      for (long long v = lo + threadIdx.x; v < hi; v += kVecThreads) {
-        const double d = -src[v];
-        const double g = A.G[base + v];
-        A.Dv[base + v] = d;
-        const double xt = A.X[base + v] + d;
-        A.XT[base + v] = xt;
-        store_trial_f32(A, P, v, xt);
-        d0 += g * d;
-        d1 += d * d;
-      }
-    } else {
-      const double t = S.t;
-      for (long long v = lo + threadIdx.x; v < hi; v += kVecThreads) {
-        const double xt = A.X[base + v] + t * A.Dv[base + v];
-        A.XT[base + v] = xt;
-        store_trial_f32(A, P, v, xt);
-      }
+    return;
+  }
+  // kFin
+  if (S.need_dir) {
+    const int h = S.hisNum;
+    if (threadIdx.x < 1 + 2 * m) s_coef[threadIdx.x] = A.coef[(size_t)p * kCoefStride + threadIdx.x];
+    __syncthreads();
+    const double gamma = s_coef[0];
+    double v[2] = {0.0, 0.0};
+    for (long long k = lo + threadIdx.x; k < hi; k += kVecThreads) {
+      const double g = A.G[base + k];
+      double hg = gamma * g;
+      if (h > 0)
+        for (int i = 0; i < m; ++i)
+          if (slot_valid(i, h, m))
+            hg += s_coef[1 + i] * A.S[(size_t)i * NV + base + k] +
+                  s_coef[1 + m + i] * A.Y[(size_t)i * NV + base + k];
+      const double d = -hg;
+      A.Dv[base + k] = d;
+      const double xt = A.X[base + k] + d;
+      A.XT[base + k] = xt;
+      store_trial_f32(A, P, k, xt);
+      v[0] += g * d;
+      v[1] += d * d;
+    }
+    block_sums<2>(v, out, 2);
+  } else {
+    const double t = S.t;
+    for (long long k = lo + threadIdx.x; k < hi; k += kVecThreads) {
+      const double xt = A.X[base + k] + t * A.Dv[base + k];
+      A.XT[base + k] = xt;
+      store_trial_f32(A, P, k, xt);
     }
   }
-  d0 = block_sum(d0, s_scr);
-  d1 = block_sum(d1, s_scr);
-  d2 = block_sum(d2, s_scr);
-  if (threadIdx.x == 0) {
-    A.part_out[(size_t)c * 3 + 0] = d0;
-    A.part_out[(size_t)c * 3 + 1] = d1;
-    A.part_out[(size_t)c * 3 + 2] = d2;
-  }
-  __syncthreads();
 }
 
 // One vector pass as its own launch (one CTA per chunk).
-__global__ void __launch_bounds__(kVecThreads) vec_pass_kernel(VecArgs A, int mode, int k) {
+__global__ void __launch_bounds__(kVecThreads) vec_pass_kernel(VecArgs A, int mode) {
   pdl_wait();
   pdl_trigger();
-  vec_pass_chunk(A, mode, k, blockIdx.x);
+  vec_pass_chunk(A, mode, blockIdx.x);
 }
 
 __device__ __forceinline__ double serial_partial(const double *part, int c0, int nc, int j) {
   double s = 0.0;
-  for (int c = 0; c < nc; ++c) s += part[(size_t)(c0 + c) * 3 + j];
+  for (int c = 0; c < nc; ++c) s += part[(size_t)(c0 + c) * kPartStride + j];
   return s;
+}
+
+// After ACCEPT, one CTA per pair with a new direction: the pair's slot dots (chunk
+// order), the S^T Y / Y^T Y update with the newest pair, the compact-form solves.
+__device__ void solve_pair(const VecArgs &A, int p) {
+  __shared__ double s_v[4 * kMaxMem];
+  PairState &S = A.st[p];
+  if (!S.need_dir) return;  // uniform for the CTA
+  const PairDesc &P = A.pd[p];
+  const int m = A.m, h = S.hisNum, nw = S.newIdx;
+  double *coef = A.coef + (size_t)p * kCoefStride;
+  if (h == 0) {  // first direction: H0 = 1 (LBFGS.cpp:73-74), d = -g
+    if (threadIdx.x == 0) {
+      coef[0] = 1.0;
+      S.H0 = 1.0;
+    }
+    return;
+  }
+  for (int j = threadIdx.x; j < 4 * m; j += blockDim.x)
+    s_v[j] = slot_valid(j / 4, h, m) ? serial_partial(A.part, P.chunk_off, P.nchunk, j) : 0.0;
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double *SY = A.SY + (size_t)p * m * m, *YY = A.YY + (size_t)p * m * m;
+  for (int i = 0; i < m; ++i) {
+    if (!slot_valid(i, h, m)) continue;
+    SY[(size_t)i * m + nw] = s_v[4 * i + 0];
+    YY[(size_t)i * m + nw] = s_v[4 * i + 1];
+    YY[(size_t)nw * m + i] = s_v[4 * i + 1];
+  }
+  const double gamma = s_v[4 * nw + 0] / s_v[4 * nw + 1];  // s.y / y.y, newest pair
+  S.H0 = gamma;
+  // chronological order of the slots, oldest first
+  int ord[kMaxMem];
+  const int old = (h < m) ? 0 : (nw + 1 == m ? 0 : nw + 1);
+  for (int a = 0; a < h; ++a) ord[a] = (old + a) % m;
+  double u[kMaxMem], w[kMaxMem];
+  // R u = S^T g  (R[a][b] = s_{o_a}.y_{o_b}, a <= b), back substitution
+  for (int a = h - 1; a >= 0; --a) {
+    double r = s_v[4 * ord[a] + 2];
+    for (int b = a + 1; b < h; ++b) r -= SY[(size_t)ord[a] * m + ord[b]] * u[b];
+    u[a] = r / SY[(size_t)ord[a] * m + ord[a]];
+  }
+  // R^T w = (D + gamma Y^T Y) u - gamma Y^T g, forward substitution
+  for (int a = 0; a < h; ++a) {
+    double t = SY[(size_t)ord[a] * m + ord[a]] * u[a] - gamma * s_v[4 * ord[a] + 3];
+    for (int b = 0; b < h; ++b) t += gamma * YY[(size_t)ord[a] * m + ord[b]] * u[b];
+    for (int b = 0; b < a; ++b) t -= SY[(size_t)ord[b] * m + ord[a]] * w[b];
+    w[a] = t / SY[(size_t)ord[a] * m + ord[a]];
+  }
+  coef[0] = gamma;
+  for (int i = 0; i < m; ++i) {
+    coef[1 + i] = 0.0;
+    coef[1 + m + i] = 0.0;
+  }
+  for (int a = 0; a < h; ++a) {
+    coef[1 + ord[a]] = w[a];
+    coef[1 + m + ord[a]] = -gamma * u[a];
+  }
+}
+
+__global__ void __launch_bounds__(kVecThreads) solve_kernel(VecArgs A) {
+  pdl_wait();
+  pdl_trigger();
+  solve_pair(A, blockIdx.x);
 }
 
 // After POST.  One thread per pair.  Records (f, |g|, step, evals) per iteration.
@@ -389,11 +417,6 @@ __global__ void ls_init_kernel(const PairDesc *__restrict__ pd, PairState *st, i
   if (p < P) ls_init_pair(pd, st, p, part, act);
 }
 
-// The whole optimiser update of one cycle in one cooperative launch: the passes of
-// the per-kernel sequence (POST, DECIDE, ACCEPT, B_0..B_{m-1}, F_0..F_{m-1}, FIN,
-// LSINIT) run as grid-stride loops over the chunks, separated by grid barriers
-// (bounded waits, persist.cuh).  Same arithmetic and reduction order as the per-kernel
-// sequence.  part[0] / part[1] alternate exactly as there.
 // Loop control of a device-side L-BFGS loop (CUDA graph WHILE node): counts the cycle
 // and keeps the loop running while some pair is active and the cycle bound is not
 // reached and no persistent sweep's barrier has timed out (error word).  Called by one
@@ -420,10 +443,13 @@ __global__ void cycle_control_kernel(cudaGraphConditionalHandle h, const int *ac
   cycle_control(h, act, P, cyc, max_cycles, sy);
 }
 
+// The whole optimiser update of one cycle in one cooperative launch: the phases of
+// the per-kernel sequence (POST, DECIDE, ACCEPT, SOLVE, FIN, LSINIT) as grid-stride
+// loops over the chunks (pairs for SOLVE), separated by grid barriers (bounded waits,
+// persist.cuh).  Same arithmetic and reduction order as the per-kernel sequence.
 __global__ void __launch_bounds__(kVecThreads)
-    lbfgs_cycle_kernel(VecArgs A, OptParams o, double *part0, double *part1, double *rec,
-                       int *act, int P, int nchunk, StepSync *sy, cudaGraphConditionalHandle h,
-                       int *cyc, int max_cycles) {
+    lbfgs_cycle_kernel(VecArgs A, OptParams o, double *rec, int *act, int P, int nchunk,
+                       StepSync *sy, cudaGraphConditionalHandle h, int *cyc, int max_cycles) {
   pdl_wait();
   stamp_entry(sy, 2);
   unsigned int phase = 0;
@@ -431,37 +457,27 @@ __global__ void __launch_bounds__(kVecThreads)
     ++phase;
     return grid_barrier(sy, phase * gridDim.x, 1000u + phase);
   };
-  int s = 0;  // pass sequence number: writes part[s & 1], reads part[(s + 1) & 1]
-  auto pass = [&](int mode, int k) {
-    A.part_out = (s & 1) ? part1 : part0;
-    A.part_in = (s & 1) ? part0 : part1;
-    for (int c = blockIdx.x; c < nchunk; c += gridDim.x) vec_pass_chunk(A, mode, k, c);
-    ++s;
+  auto pass = [&](int mode) {
+    for (int c = blockIdx.x; c < nchunk; c += gridDim.x) vec_pass_chunk(A, mode, c);
   };
   bool ok = true;
   do {  // one pass; a timed-out barrier breaks out to the loop-control exit below
-    pass(kPost, 0);
+    pass(kPost);
     if (!(ok = barrier())) break;
     if (blockIdx.x == 0)
-      for (int p = threadIdx.x; p < P; p += blockDim.x) decide_pair(A.pd, A.st, p, part0, o, rec);
+      for (int p = threadIdx.x; p < P; p += blockDim.x) decide_pair(A.pd, A.st, p, A.part, o, rec);
     if (!(ok = barrier())) break;
-    pass(kAccept, 0);
+    pass(kAccept);
     if (!(ok = barrier())) break;
-    for (int k = 0; k < o.mem_num && ok; ++k) {
-      pass(kTwoLoopB, k);
-      ok = barrier();
+    for (int p = blockIdx.x; p < P; p += gridDim.x) {
+      solve_pair(A, p);
+      __syncthreads();
     }
-    for (int k = 0; k < o.mem_num && ok; ++k) {
-      pass(kTwoLoopF, k);
-      ok = barrier();
-    }
-    if (!ok) break;
-    pass(kFin, 0);
     if (!(ok = barrier())) break;
-    if (blockIdx.x == 0) {
-      const double *last = ((s - 1) & 1) ? part1 : part0;
-      for (int p = threadIdx.x; p < P; p += blockDim.x) ls_init_pair(A.pd, A.st, p, last, act);
-    }
+    pass(kFin);
+    if (!(ok = barrier())) break;
+    if (blockIdx.x == 0)
+      for (int p = threadIdx.x; p < P; p += blockDim.x) ls_init_pair(A.pd, A.st, p, A.part, act);
   } while (false);
   if (ok) grid_depart(sy);
   if (blockIdx.x == 0 && cyc) {

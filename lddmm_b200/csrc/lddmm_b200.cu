@@ -164,10 +164,11 @@ struct lddmm_ctx {
   double *reg_part = nullptr, *vfd_part = nullptr, *f_dev = nullptr;
   int2 *pt_items = nullptr, *el_items = nullptr;
   int *chunk_pair = nullptr;
-  double *X = nullptr, *G = nullptr, *XT = nullptr, *GT = nullptr, *Dv = nullptr, *Qv = nullptr;
+  double *X = nullptr, *G = nullptr, *XT = nullptr, *GT = nullptr, *Dv = nullptr;
   double *Sh = nullptr, *Yh = nullptr;
+  double *SYm = nullptr, *YYm = nullptr, *coef = nullptr;  // compact-form L-BFGS state
   int m_alloc = 0;
-  double *part[2] = {nullptr, nullptr};
+  double *part = nullptr;
   double *rec = nullptr;
   int rec_cap = 0;
 
@@ -216,8 +217,9 @@ lddmm_ctx::~lddmm_ctx() {
   dfree(pt_pair, stream); dfree(adj_ptr, stream); dfree(adj, stream); dfree(reg_part, stream);
   dfree(vfd_part, stream); dfree(f_dev, stream); dfree(pt_items, stream);
   dfree(el_items, stream); dfree(chunk_pair, stream); dfree(X, stream); dfree(G, stream);
-  dfree(XT, stream); dfree(GT, stream); dfree(Dv, stream); dfree(Qv, stream);
-  dfree(Sh, stream); dfree(Yh, stream); dfree(part[0], stream); dfree(part[1], stream);
+  dfree(XT, stream); dfree(GT, stream); dfree(Dv, stream);
+  dfree(Sh, stream); dfree(Yh, stream); dfree(part, stream);
+  dfree(SYm, stream); dfree(YYm, stream); dfree(coef, stream);
   dfree(rec, stream); dfree(sync, stream); dfree(units, stream); dfree(segs, stream);
   dfree(cta_seg, stream); dfree(unit_parts, stream); dfree(seg_part, stream);
   dfree(unit_cnt, stream);
@@ -913,8 +915,7 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   CU(dalloc(c.stream, &c.chunk_pair, c.nchunk_tot));
   CU(dalloc(c.stream, &c.XT, c.nvar));
   CU(dalloc(c.stream, &c.GT, c.nvar));
-  CU(dalloc(c.stream, &c.part[0], (size_t)c.nchunk_tot * 3));
-  CU(dalloc(c.stream, &c.part[1], (size_t)c.nchunk_tot * 3));
+  CU(dalloc(c.stream, &c.part, (size_t)c.nchunk_tot * kPartStride));
 
   CU(cudaMemcpyAsync(c.qs, h_qs.data(), sizeof(float4) * c.NPtot,
                      cudaMemcpyHostToDevice, c.stream));
@@ -1225,13 +1226,17 @@ static cudaError_t ensure_lbfgs_buffers(lddmm_ctx &c, int m, int rec_cap) {
     CUE(dalloc(c.stream, &c.X, c.nvar));
     CUE(dalloc(c.stream, &c.G, c.nvar));
     CUE(dalloc(c.stream, &c.Dv, c.nvar));
-    CUE(dalloc(c.stream, &c.Qv, c.nvar));
+    CUE(dalloc(c.stream, &c.coef, (size_t)c.P * kCoefStride));
   }
   if (c.m_alloc < m) {
     dfree(c.Sh, c.stream);
     dfree(c.Yh, c.stream);
+    dfree(c.SYm, c.stream);
+    dfree(c.YYm, c.stream);
     CUE(dalloc(c.stream, &c.Sh, (size_t)m * c.nvar));
     CUE(dalloc(c.stream, &c.Yh, (size_t)m * c.nvar));
+    CUE(dalloc(c.stream, &c.SYm, (size_t)c.P * m * m));
+    CUE(dalloc(c.stream, &c.YYm, (size_t)c.P * m * m));
     c.m_alloc = m;
     c.graph_valid = false;
   }
@@ -1253,8 +1258,10 @@ static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o,
   A.pd = c.pd;
   A.st = c.st;
   A.chunk_pair = c.chunk_pair;
-  A.X = c.X; A.G = c.G; A.XT = c.XT; A.GT = c.GT; A.Dv = c.Dv; A.Qv = c.Qv;
+  A.X = c.X; A.G = c.G; A.XT = c.XT; A.GT = c.GT; A.Dv = c.Dv;
   A.S = c.Sh; A.Y = c.Yh;
+  A.part = c.part;
+  A.SY = c.SYm; A.YY = c.YYm; A.coef = c.coef;
   A.nvar = c.nvar;
   A.as = c.as;
   A.NPtot = c.NPtot;
@@ -1273,39 +1280,33 @@ static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o,
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, lbfgs_cycle_kernel, A, o, c.part[0], c.part[1], c.rec, c.act,
+    return cudaLaunchKernelEx(&cfg, lbfgs_cycle_kernel, A, o, c.rec, c.act,
                               c.P, c.nchunk_tot, c.sync, h, max_cycles > 0 ? c.cyc : nullptr,
                               max_cycles);
   }
-  int s = 0;  // pass sequence number: writes part[s & 1], reads part[(s - 1) & 1]
-  auto pass = [&](int mode, int k) -> cudaError_t {
-    A.part_out = c.part[s & 1];
-    A.part_in = c.part[(s + 1) & 1];
-    const cudaError_t e = launch(vec_pass_kernel, nb, kVecThreads, 0, c.stream, A, mode, k);
-    ++s;
-    return e;
+  auto pass = [&](int mode) -> cudaError_t {
+    return launch(vec_pass_kernel, nb, kVecThreads, 0, c.stream, A, mode);
   };
-  CUE(pass(kPost, 0));
+  CUE(pass(kPost));
   CUE(launch(decide_kernel, (unsigned)pb, 128, 0, c.stream, (const PairDesc *)c.pd, c.st, c.P,
-             (const double *)c.part[0], o, c.rec));
-  CUE(pass(kAccept, 0));
-  for (int k = 0; k < o.mem_num; ++k) CUE(pass(kTwoLoopB, k));
-  for (int k = 0; k < o.mem_num; ++k) CUE(pass(kTwoLoopF, k));
-  CUE(pass(kFin, 0));
+             (const double *)c.part, o, c.rec));
+  CUE(pass(kAccept));
+  CUE(launch(solve_kernel, (unsigned)c.P, kVecThreads, 0, c.stream, A));
+  CUE(pass(kFin));
   CUE(launch(ls_init_kernel, (unsigned)pb, 128, 0, c.stream, (const PairDesc *)c.pd, c.st, c.P,
-             (const double *)c.part[(s - 1) & 1], c.act));
+             (const double *)c.part, c.act));
   if (max_cycles > 0)
     CUE(launch(cycle_control_kernel, 1, 256, 0, c.stream, h, (const int *)c.act, c.P, c.cyc,
                max_cycles, (const StepSync *)c.sync));
   return cudaSuccess;
 }
 
-static long long kernels_per_cycle(const lddmm_ctx &c, int m) {
+static long long kernels_per_cycle(const lddmm_ctx &c) {
   // objective: T shooting + [geometry + varifold] + gather + objective + T adjoint
   // (2 launches when the time loops are persistent); optimiser: POST, DECIDE, ACCEPT,
-  // m + m two-loop passes, FIN, LSINIT (1 launch when fused)
+  // SOLVE, FIN, LSINIT (1 launch when fused)
   const long long sweeps = c.persistent ? 2 : 2LL * c.T;
-  const long long opt = c.cycle_grid > 0 ? 1 : 2LL * m + 5;
+  const long long opt = c.cycle_grid > 0 ? 1 : 6;
   return sweeps + 2 + (c.has_vfd ? 2 : 0) + opt;
 }
 
@@ -1483,7 +1484,7 @@ static int lbfgs_run(lddmm_ctx &c, const lddmm_opt *opt, const double *alp, bool
     }
   }
   c.last_cycles = cycles;
-  c.last_launches = cycles * kernels_per_cycle(c, o.mem_num) + 2;
+  c.last_launches = cycles * kernels_per_cycle(c) + 2;
   CU(cudaMemcpyAsync(hs.data(), c.st, sizeof(PairState) * c.P, cudaMemcpyDeviceToHost, c.stream));
   CU(cudaMemcpyAsync(alp_out, c.X, sizeof(double) * c.nvar,
                      host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, c.stream));
@@ -1572,7 +1573,7 @@ extern "C" int lddmm_ctx_counters(const lddmm_ctx *ctx, long long *out, int n) {
                           ctx->last_launches, ctx->last_evals};
   const int k = std::min(n, 4);
   for (int i = 0; i < k; ++i) out[i] = v[i];
-  if (k >= 2 && ctx->last_cycles) out[1] = kernels_per_cycle(*ctx, ctx->graph_opt.mem_num);
+  if (k >= 2 && ctx->last_cycles) out[1] = kernels_per_cycle(*ctx);
   return k;
 }
 

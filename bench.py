@@ -57,9 +57,12 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--itr", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["registration", "objgrd"], default="registration",
+    ap.add_argument("--mode", choices=["registration", "objgrd", "large_pair"],
+                    default="registration",
                     help="objgrd: only time device-resident objective+gradient evaluations "
-                         "(the command the ncu captures in profiles/ use)")
+                         "(the command the ncu captures in profiles/ use); large_pair: the "
+                         "163,842-landmark star-surface pair, --itr L-BFGS iterations "
+                         "timed (default 100)")
     ap.add_argument("--evals", type=int, default=20)
     ap.add_argument("--subdiv", type=int, default=4,
                     help="objgrd mode: icosphere subdivisions of the source (4: 2562 points)")
@@ -470,10 +473,67 @@ def run_objgrd(args):
     ctx.close()
 
 
+def run_large_pair(args):
+    """One large pair: a star-shaped surface on the 7-times subdivided icosphere
+    (163,842 landmarks, 327,680 triangles) onto a star-shaped target on the 6-times
+    subdivided icosphere (81,920 triangles), Gaussian 0.3, varifold Gaussian 0.1 x
+    Binet, T = 10.  Times ``--itr`` L-BFGS iterations from zero momenta (CUDA events
+    on the context stream; tolerance 0 so every iteration runs) and the sweeps of one
+    evaluation; prints one JSON line."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from lddmm_b200 import _lib, api, problem
+
+    itr = args.itr if args.itr != 500 else 100
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    P = problem.star_pair()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx = api.Context(P, stream=stream.cuda_stream)
+    sweeps = ctx.time_sweeps(reps=2)
+    peak = C.c_double()
+    _lib.check(_lib.lib.lddmm_fp32_peak(local, C.byref(peak)))
+    T, N, Ed, Et = P.T, P.nde_num, P.dfm_elm_num, P.tgt_elm_num
+    pairs_launch = {"shoot": N * N, "adjoint": N * N, "varifold": Ed * (Ed + Et)}
+    frac = {}
+    for i, k in enumerate(("shoot", "adjoint", "varifold")):
+        fl = _lib.lib.lddmm_flops_per_pair(i, 3, P.knl_order, b"G", b"B")
+        tf = pairs_launch[k] * fl / (sweeps[k] * 1e-3) / 1e12
+        frac[k] = {"ms": sweeps[k], "flops_per_pair": fl, "tflops": tf,
+                   "frac_of_measured_fp32": tf / peak.value}
+    x0 = np.zeros(ctx.var_total)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        _, res = ctx.lbfgs(x0, itr_max=itr, tol=0.0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    s = e0.elapsed_time(e1) * 1e-3
+    r = res[0]
+    pairs_eval = 2 * T * N * N + Ed * (Ed + Et)
+    print(json.dumps({
+        "mode": "large_pair", "landmarks": N, "triangles": Ed, "target_triangles": Et,
+        "time_steps": T, "iterations": r["iters"], "evaluations": r["evals"],
+        "status": r["status"], "f": r["f"], "seconds": s,
+        "ms_per_evaluation": s * 1e3 / max(r["evals"], 1),
+        "gpair_interactions_per_s": (r["evals"] * pairs_eval + Et * Et) / s / 1e9,
+        "sweeps": frac, "fp32_peak_tflops": peak.value, "clocks": clk.summary()}),
+        flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
     if args.mode == "objgrd":
         run_objgrd(args)
+        return
+    if args.mode == "large_pair":
+        run_large_pair(args)
         return
     if args.impl == "reference":
         run_reference(args)

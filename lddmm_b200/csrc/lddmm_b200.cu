@@ -605,7 +605,7 @@ struct HostPlan {
   int slots = 0;
 };
 
-constexpr long long kMinPart = 128;
+constexpr long long kMinPart = 32;
 constexpr long long kSplitMin = 512;
 
 static HostPlan plan_sweeps(const std::vector<int2> &units, const std::vector<PairDesc> &hpd,

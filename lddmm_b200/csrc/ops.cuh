@@ -233,9 +233,10 @@ struct AdjointOp {
       acc[D + d] = fmaf(s, dq[d], acc[D + d]);
     }
   }
-  // finalize operand loaded before the row sums are complete: p of the row
+  // finalize operands loaded before the row sums are complete: p of the row and, when
+  // the next step's u / l are formed, a_{t-1} of the row
   struct FData {
-    double p[3];
+    double p[3], a[3];
   };
   __device__ void fin_load(int p, int row, FData &F) const {
     const PairDesc &P = pd[p];
@@ -243,6 +244,11 @@ struct AdjointOp {
     const size_t g = (size_t)P.pt_off + row;
 #pragma unroll
     for (int d = 0; d < D; ++d) F.p[d] = __ldcg(&p64[g * D + d]);
+    if (t > 0 && us_n) {
+      const double *a = x64 + P.var_off + ((size_t)(t - 1) * P.N + row) * D;
+#pragma unroll
+      for (int d = 0; d < D; ++d) F.a[d] = __ldcg(&a[d]);
+    }
   }
   __device__ double finalize(int p, int row, const double (&v)[NA], const FData &F) const {
     const PairDesc &P = pd[p];
@@ -258,12 +264,11 @@ struct AdjointOp {
       p64[g * D + d] = pn[d];
     }
     if (t > 0 && us_n) {
-      const double *a = x64 + P.var_off + ((size_t)(t - 1) * P.N + row) * D;
       double u[3] = {0.0, 0.0, 0.0}, l[3] = {0.0, 0.0, 0.0};
 #pragma unroll
       for (int d = 0; d < D; ++d) {
-        u[d] = a[d] - pn[d];
-        l[d] = 0.5 * a[d] - pn[d];
+        u[d] = F.a[d] - pn[d];
+        l[d] = 0.5 * F.a[d] - pn[d];
       }
       us_n[g] = make_float4((float)u[0], (float)u[1], (float)u[2], 0.0f);
       ls_n[g] = make_float4((float)l[0], (float)l[1], (float)l[2], 0.0f);

@@ -14,12 +14,14 @@
 //     of pair interactions whatever the row-group count, so no SM idles at the barrier
 //     while another runs a second row group.  A CTA's share is a list of segments
 //     (row group, j range), taken two at a time ("rounds");
-//   * in a round the 8 warps are dealt to the (one or two) segments in proportion to
-//     their lengths and take equal contiguous shares of their segment's j range; lane
-//     l handles rows l % 8 and l % 8 + 8 against every 4th point of each staged
-//     32-point sub-tile (lane group l / 8), so each staged operand serves two pairs;
-//   * reductions: a shuffle butterfly over the 4 lane groups, then the segment's warps
-//     through shared memory in warp order, in FP64 after the per-tile TwoSum.  A row
+//   * in a round the entries of its (one or two) segments, laid end to end, are cut
+//     into 8 equal contiguous warp shares (a share that straddles the two segments is
+//     processed as two pieces); lane l handles rows l % 8 and l % 8 + 8 against every
+//     4th point of each staged 32-point sub-tile (lane group l / 8), so each staged
+//     operand serves two pairs;
+//   * reductions: a shuffle butterfly over the 4 lane groups, then all 8 warps through
+//     shared memory in warp order (a warp without entries of the segment adds zero),
+//     in FP64 after the per-tile TwoSum.  A row
 //     group cut over several CTAs stores one FP64 partial per part; the CTA that
 //     completes the row group's arrival count (whichever it is) adds the parts in part
 //     order and finalises, so results are bit-reproducible for a given plan;
@@ -74,6 +76,13 @@ __device__ __forceinline__ void stamp_exit(StepSync *sy, int slot) {
 
 constexpr unsigned int kSpinLimit = 1u << 23;  // polls: a few seconds at most
 
+// Release / acquire fence at GPU scope: orders this thread's (and, cumulatively, its
+// CTA's synchronised) writes before a later relaxed atomic, and an observed atomic
+// before later reads.  Lighter than the sequentially consistent __threadfence().
+__device__ __forceinline__ void fence_acq_rel_gpu() {
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+}
+
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
   unsigned int v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -98,7 +107,7 @@ __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    __threadfence();
+    fence_acq_rel_gpu();
     atomicAdd(&sy->arrive, 1u);
     unsigned int n = 0;
     while (ld_relaxed(&sy->arrive) < target) {
@@ -111,7 +120,7 @@ __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
         if (n > 4096u) __nanosleep(64);
       }
     }
-    __threadfence();
+    fence_acq_rel_gpu();
     s_ok = ok;
   }
   __syncthreads();
@@ -154,9 +163,10 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 2)
   constexpr int NW = kPersistWarps;
   static_assert(NA <= kPartNA, "partial slot too small");
   __shared__ float4 s_j[NW][JW][kSub];
-  __shared__ double s_red[NW][kGroup][NA];
+  __shared__ double s_red[2][NW][kGroup][NA];  // [segment of the round][warp][row]
   __shared__ PairDesc s_pd[2];  // descriptors of the round's units
   __shared__ int s_uinf[2][2];  // per round slot: pair | group << 16, active
+  __shared__ int4 s_seg[2];     // the round's segments
   pdl_wait();
   stamp_entry(sy, dir > 0 ? 0 : 1);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -169,27 +179,37 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 2)
     o.set_step(t);
     for (int k = s0; k < s1; k += 2) {
       const int nseg = min(2, s1 - k);
-      const int4 sa = plan.segs[k];
-      const int4 sb = nseg > 1 ? plan.segs[k + 1] : make_int4(0, 0, 0, 0);
       if (!one_round || s == 0) {
-        __syncthreads();  // the previous round's epilogue is done with s_pd / s_uinf
+        __syncthreads();  // the previous round's epilogue is done with the round slots
         if (threadIdx.x < nseg) {
-          const int2 un = plan.units[threadIdx.x == 0 ? sa.x : sb.x];
+          const int4 sg = plan.segs[k + threadIdx.x];
+          const int2 un = plan.units[sg.x];
+          s_seg[threadIdx.x] = sg;
           s_uinf[threadIdx.x][0] = un.x | (un.y << 16);
           s_uinf[threadIdx.x][1] = op.active(un.x);
           s_pd[threadIdx.x] = op.pd[un.x];
         }
         __syncthreads();
       }
-      // warps dealt to the segments in proportion to their lengths (>= 1 each)
-      const int la = sa.z - sa.y, lb = nseg > 1 ? sb.z - sb.y : 0;
-      const int wa = nseg > 1 ? min(NW - 1, max(1, (int)((2LL * NW * la + la + lb) /
-                                                           (2LL * (la + lb)))))
-                              : NW;
-      const int g = warp < wa ? 0 : 1;  // this warp's segment (warp-uniform)
-      if (s_uinf[g][1]) {
-        const int4 sg = g ? sb : sa;
-        const int wl = g ? warp - wa : warp, nw = g ? NW - wa : wa;
+      // the round's entries (segment a, then segment b) cut into NW equal contiguous
+      // warp shares; a share that straddles the two segments is processed as two
+      // pieces, one per segment
+      const int la = s_seg[0].z - s_seg[0].y, lb = nseg > 1 ? s_seg[1].z - s_seg[1].y : 0;
+      const int wb = (int)((long long)(la + lb) * warp / NW);
+      const int we = (int)((long long)(la + lb) * (warp + 1) / NW);
+#pragma unroll 1
+      for (int g = 0; g < nseg; ++g) {
+        const int off = g ? la : 0, len = g ? lb : la;
+        const int lo = max(wb, off), hi = min(we, off + len);
+        if (hi <= lo || !s_uinf[g][1]) {
+          // no entries of this segment: a zero contribution to its warp-order sum
+          if (lane < kGroup) {
+#pragma unroll
+            for (int a = 0; a < NA; ++a) s_red[g][warp][lane][a] = 0.0;
+          }
+          continue;
+        }
+        const int4 sg = s_seg[g];
         const int grp = s_uinf[g][0] >> 16;
         o.pd = &s_pd[g];  // the op reads descriptor 0 from shared memory from here on
         const int p = 0;
@@ -199,9 +219,8 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 2)
         float hi0[NA], lo0[NA], hi1[NA], lo1[NA];
 #pragma unroll
         for (int a = 0; a < NA; ++a) hi0[a] = lo0[a] = hi1[a] = lo1[a] = 0.0f;
-        const int L = sg.z - sg.y;
-        const int jb = sg.y + (int)((long long)L * wl / nw);
-        const int je = sg.y + (int)((long long)L * (wl + 1) / nw);
+        const int jb = sg.y + (lo - off);
+        const int je = sg.y + (hi - off);
         const int split = Op::kTwoSets ? o.set_boundary(p) : sg.z;
         float4 nxt[JW];
         float acc0[NA], acc1[NA];
@@ -256,13 +275,13 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 2)
           double v0 = (double)hi0[a] + (double)lo0[a];
           double v1 = (double)hi1[a] + (double)lo1[a];
 #pragma unroll
-          for (int off = kRowPairs; off < 32; off <<= 1) {
-            v0 += __shfl_xor_sync(0xffffffffu, v0, off);
-            v1 += __shfl_xor_sync(0xffffffffu, v1, off);
+          for (int off2 = kRowPairs; off2 < 32; off2 <<= 1) {
+            v0 += __shfl_xor_sync(0xffffffffu, v0, off2);
+            v1 += __shfl_xor_sync(0xffffffffu, v1, off2);
           }
           if (lg == 0) {
-            s_red[warp][lrow][a] = v0;
-            s_red[warp][kRowPairs + lrow][a] = v1;
+            s_red[g][warp][lrow][a] = v0;
+            s_red[g][warp][kRowPairs + lrow][a] = v1;
           }
         }
       }
@@ -271,20 +290,22 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 2)
       // condition is uniform over those 16 lanes
       const int e = warp;
       if (e < nseg && lane < kGroup && s_uinf[e][1]) {
-        const int4 se = e ? sb : sa;
-        const int w0 = e ? wa : 0, w1 = e ? NW : wa;
+        const int4 se = s_seg[e];
         const int grp_e = s_uinf[e][0] >> 16;
         Op &oe = o;
         oe.pd = &s_pd[e];
+        typename Op::FData F;  // finalize operands, in flight during the combine
+        oe.fin_load(0, grp_e * kGroup + lane, F);
         double v[NA];
 #pragma unroll
         for (int a = 0; a < NA; ++a) {
+          // all NW warps in warp order (zeros from warps without entries here); the
+          // loads are independent of the running sum
           double x = 0.0;
-          for (int w = w0; w < w1; ++w) x += s_red[w][lane][a];
+#pragma unroll
+          for (int w = 0; w < NW; ++w) x += s_red[e][w][lane][a];
           v[a] = x;
         }
-        typename Op::FData F;  // finalize operands, in flight during the combine
-        oe.fin_load(0, grp_e * kGroup + lane, F);
         const int2 up = plan.unit_parts[se.x];
         bool fin = true;
         if (up.x > 1) {
@@ -293,14 +314,14 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 2)
           double *slot = plan.part + ((size_t)(up.y + se.w) * kGroup + lane) * kPartNA;
 #pragma unroll
           for (int a = 0; a < NA; ++a) slot[a] = v[a];
-          __threadfence();
+          fence_acq_rel_gpu();
           __syncwarp(0xffffu);
           int last = 0;
           if (lane == 0) {
             last = atomicAdd(&plan.cnt[se.x], 1u) == (unsigned int)up.x - 1u;
             if (last) {
               plan.cnt[se.x] = 0u;  // next step's arrivals come after the grid barrier
-              __threadfence();
+              fence_acq_rel_gpu();
             }
           }
           fin = __shfl_sync(0xffffu, last, 0) != 0;

@@ -18,6 +18,10 @@
  *   lddmm_elm_ifo     <- getElmIfo.m                               Cpp/src/getElmIfo.m:1
  *   lddmm_multiply_kernel <- multiplyKernel (MEX multiplyKernelITF) Cpp/src/multiplyKernel.cpp:22
  *   lddmm_dq_kernel   <- dqKernel                                  Cpp/src/dqKernel.cpp:31
+ *   lddmm_compute_kernel, lddmm_multiply_kernel2, lddmm_dq_kernel2
+ *                     <- the two-set computeKernel / multiplyKernel / dqKernel
+ *                        overloads  Cpp/src/computeKernel.cpp:246, multiplyKernel.cpp:294,
+ *                        dqKernel.cpp:307
  *   lddmm_varifold    <- varifoldITF / varifold (gradient overload) Cpp/src/varifoldITF.cpp:7
  *
  * Layout is the reference's C++ one: coordinates fastest, then node, then time
@@ -189,6 +193,28 @@ int lddmm_multiply_kernel(int dim, int n, const double *q, const double *a, int 
 int lddmm_dq_kernel(int dim, int n, const double *q, const double *l, const double *r,
                     int knl_order, double knl_width, double *dq);
 int lddmm_varifold(const lddmm_problem *prob, const double *nde, double *val, double *dq);
+
+/* Two landmark sets (the reference's two-set overloads, reached through the MEX
+ * interfaces computeKernelITF / multiplyKernelITF / dqKernelITF with 4 / 5 / 6
+ * inputs).  qi: dim x ni, qj: dim x nj, C++ layout; host buffers; any kernel order
+ * (-1 Gaussian, 0..4 Matern) in 2D and 3D.
+ *
+ * Dense kernel matrix, the reference's column-major ni x nj layout
+ * knl[j * ni + i] = K(qi_i, qj_j); qj == NULL gives the one-set matrix of qi
+ * (nj is then ignored)  <- computeKernel, Cpp/src/computeKernel.cpp:246 and :21.
+ * FP32 evaluation stored as FP64 (relative error ~1e-7 of the largest entry). */
+int lddmm_compute_kernel(int dim, int ni, const double *qi, int nj, const double *qj,
+                         int knl_order, double knl_width, double *knl);
+/* v_i = sum_j K(qi_i, qj_j) a_j, a: dim x nj, v: dim x ni
+ *                                  <- multiplyKernel, Cpp/src/multiplyKernel.cpp:294 */
+int lddmm_multiply_kernel2(int dim, int ni, const double *qi, int nj, const double *qj,
+                           const double *a, int knl_order, double knl_width, double *v);
+/* l: dim x ni, r: dim x nj;
+ * dqi_i = sum_j (l_i.r_j) dK(qi_i, qj_j)/dqi_i, dqj_j = sum_i (l_i.r_j) dK/dqj_j
+ *                                  <- dqKernel, Cpp/src/dqKernel.cpp:307 */
+int lddmm_dq_kernel2(int dim, int ni, const double *qi, int nj, const double *qj,
+                     const double *l, const double *r, int knl_order, double knl_width,
+                     double *dqi, double *dqj);
 
 /* Allocation-free v_i = sum_j K(q_i, q_j) a_j.  No counterpart in the reference.
  *

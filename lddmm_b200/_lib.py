@@ -26,7 +26,8 @@ EXPORTS = [
     "lddmm_fp32_peak", "lddmm_multiply_kernel_noalloc", "lddmm_ctx_timeline",
     "lddmm_ws_create", "lddmm_ws_destroy", "lddmm_ws_last_error", "lddmm_ws_num_params",
     "lddmm_ws_params", "lddmm_ws_grad", "lddmm_ws_train_step", "lddmm_ws_predict",
-    "lddmm_ws_gemm_bf16", "lddmm_wait_selftest",
+    "lddmm_ws_gemm_bf16", "lddmm_wait_selftest", "lddmm_compute_kernel",
+    "lddmm_multiply_kernel2", "lddmm_dq_kernel2",
 ]
 
 ERRORS = {
@@ -101,6 +102,12 @@ def _load():
     L.lddmm_elm_ifo.argtypes = [_ip, C.c_int, C.c_int, C.c_int, _ip]
     L.lddmm_multiply_kernel.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_int, C.c_double, _dp]
     L.lddmm_dq_kernel.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, C.c_int, C.c_double, _dp]
+    L.lddmm_compute_kernel.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _dp, C.c_int,
+                                       C.c_double, _dp]
+    L.lddmm_multiply_kernel2.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _dp, _dp, C.c_int,
+                                         C.c_double, _dp]
+    L.lddmm_dq_kernel2.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _dp, _dp, _dp, C.c_int,
+                                   C.c_double, _dp, _dp]
     L.lddmm_varifold.argtypes = [C.POINTER(Problem), _dp, _dp, _dp]
     L.lddmm_flops_per_pair.argtypes = [C.c_int, C.c_int, C.c_int, C.c_char, C.c_char]
     L.lddmm_flops_per_pair.restype = C.c_double

@@ -158,23 +158,70 @@ def objgrd(P: Problem, alp):
     return float(f[0]), g
 
 
-def multiplyKernel(q, a, knl_order, knl_width):
-    """v_i = sum_j K(q_i, q_j) a_j (Cpp/src/multiplyKernel.cpp:22); q, a: (N, D)."""
-    q = np.ascontiguousarray(q, dtype=np.float64)
-    a = np.ascontiguousarray(a, dtype=np.float64)
-    v = np.zeros_like(q)
-    check(lib.lddmm_multiply_kernel(q.shape[1], q.shape[0], dptr(q), dptr(a), knl_order,
-                                    knl_width, dptr(v)))
-    return v
+def _pts(x):
+    return np.ascontiguousarray(x, dtype=np.float64)
 
 
-def dqKernel(q, l, r, knl_order, knl_width):
-    """dq_i = sum_j (l_i.r_j + l_j.r_i) dK/dq_i (Cpp/src/dqKernel.cpp:31)."""
-    q, l, r = (np.ascontiguousarray(x, dtype=np.float64) for x in (q, l, r))
-    dq = np.zeros_like(q)
-    check(lib.lddmm_dq_kernel(q.shape[1], q.shape[0], dptr(q), dptr(l), dptr(r), knl_order,
-                              knl_width, dptr(dq)))
-    return dq
+def computeKernel(*args):
+    """Dense kernel matrix, as the MEX ``computeKernel`` (MATLAB/src/computeKernelITF.cpp):
+    ``computeKernel(lmk, knl_order, knl_width)`` -> (N, N), or
+    ``computeKernel(lmki, lmkj, knl_order, knl_width)`` -> (Ni, Nj) with entry (i, j) =
+    K(lmki_i, lmkj_j) (Cpp/src/computeKernel.cpp:21 and :246).  Points are (N, D)."""
+    if len(args) == 3:
+        qi, qj, (order, width) = _pts(args[0]), None, args[1:]
+    elif len(args) == 4:
+        qi, qj, (order, width) = _pts(args[0]), _pts(args[1]), args[2:]
+    else:
+        raise TypeError("computeKernel takes 3 or 4 arguments")
+    nj = qi.shape[0] if qj is None else qj.shape[0]
+    K = np.zeros((nj, qi.shape[0]))  # the reference's column-major Ni x Nj
+    check(lib.lddmm_compute_kernel(qi.shape[1], qi.shape[0], dptr(qi), nj,
+                                   None if qj is None else dptr(qj), order, width, dptr(K)))
+    return K.T.copy()
+
+
+def multiplyKernel(*args):
+    """As the MEX ``multiplyKernel`` (MATLAB/src/multiplyKernelITF.cpp):
+    ``multiplyKernel(q, a, knl_order, knl_width)``: v_i = sum_j K(q_i, q_j) a_j
+    (Cpp/src/multiplyKernel.cpp:22); ``multiplyKernel(qi, qj, a, knl_order, knl_width)``:
+    v_i = sum_j K(qi_i, qj_j) a_j with a on the j set (multiplyKernel.cpp:294).
+    Points and vectors are (N, D)."""
+    if len(args) == 4:
+        q, a, order, width = _pts(args[0]), _pts(args[1]), args[2], args[3]
+        v = np.zeros_like(q)
+        check(lib.lddmm_multiply_kernel(q.shape[1], q.shape[0], dptr(q), dptr(a), order,
+                                        width, dptr(v)))
+        return v
+    if len(args) == 5:
+        qi, qj, a, order, width = _pts(args[0]), _pts(args[1]), _pts(args[2]), args[3], args[4]
+        v = np.zeros_like(qi)
+        check(lib.lddmm_multiply_kernel2(qi.shape[1], qi.shape[0], dptr(qi), qj.shape[0],
+                                         dptr(qj), dptr(a), order, width, dptr(v)))
+        return v
+    raise TypeError("multiplyKernel takes 4 or 5 arguments")
+
+
+def dqKernel(*args):
+    """As the MEX ``dqKernel`` (MATLAB/src/dqKernelITF.cpp):
+    ``dqKernel(q, l, r, knl_order, knl_width)``: dq_i = sum_j (l_i.r_j + l_j.r_i) dK/dq_i
+    (Cpp/src/dqKernel.cpp:31); ``dqKernel(qi, qj, l, r, knl_order, knl_width)`` ->
+    (dqi, dqj), the gradients of sum_ij l_i.r_j K(qi_i, qj_j) with respect to qi and qj,
+    l on the i set, r on the j set (dqKernel.cpp:307)."""
+    if len(args) == 5:
+        q, l, r = (_pts(x) for x in args[:3])
+        order, width = args[3], args[4]
+        dq = np.zeros_like(q)
+        check(lib.lddmm_dq_kernel(q.shape[1], q.shape[0], dptr(q), dptr(l), dptr(r), order,
+                                  width, dptr(dq)))
+        return dq
+    if len(args) == 6:
+        qi, qj, l, r = (_pts(x) for x in args[:4])
+        order, width = args[4], args[5]
+        dqi, dqj = np.zeros_like(qi), np.zeros_like(qj)
+        check(lib.lddmm_dq_kernel2(qi.shape[1], qi.shape[0], dptr(qi), qj.shape[0], dptr(qj),
+                                   dptr(l), dptr(r), order, width, dptr(dqi), dptr(dqj)))
+        return dqi, dqj
+    raise TypeError("dqKernel takes 5 or 6 arguments")
 
 
 def varifold(P: Problem, nde):

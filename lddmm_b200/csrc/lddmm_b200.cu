@@ -13,6 +13,7 @@
 
 #include "../../include/lddmm_b200.h"
 #include "common.cuh"
+#include "cross.cuh"
 #include "kernels.cuh"
 #include "layout.h"
 #include "lbfgs.cuh"
@@ -1786,6 +1787,230 @@ extern "C" int lddmm_dq_kernel(int dim, int n, const double *q, const double *l,
   CU(cudaMemcpyAsync(h.data(), pd, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c.stream));
   CU(cudaStreamSynchronize(c.stream));
   std::memcpy(dq, h.data() + (size_t)P.pt_off * dim, sizeof(double) * n * dim);
+  return 0;
+}
+
+// ============================================================ two point sets
+
+namespace {
+
+// One call's device work on its own stream, with every buffer from the device's
+// stream-ordered pool; the destructor releases them and the stream.
+struct OneShot {
+  cudaStream_t st = nullptr;
+  std::vector<void *> bufs;
+  ~OneShot() {
+    for (void *p : bufs) cudaFreeAsync(p, st);
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
+  }
+  cudaError_t init() { return cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking); }
+  template <class T>
+  cudaError_t alloc(T **p, size_t n) {
+    const cudaError_t e = dalloc(st, p, std::max<size_t>(n, 1));
+    if (e == cudaSuccess) bufs.push_back((void *)*p);
+    return e;
+  }
+  // n points (dim coordinates each, times `scale`) as FP32 float4, zero-padded to npad
+  cudaError_t put_points(float4 **d, const double *x, int n, int npad, int dim, double scale) {
+    std::vector<float4> h((size_t)npad, make_float4(0, 0, 0, 0));
+    for (int i = 0; i < n; ++i) {
+      float c[3] = {0, 0, 0};
+      for (int k = 0; k < dim; ++k) c[k] = (float)(x[(size_t)i * dim + k] * scale);
+      h[i] = make_float4(c[0], c[1], c[2], 0.0f);
+    }
+    cudaError_t e = alloc(d, (size_t)npad);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(*d, h.data(), sizeof(float4) * npad, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // h goes out of scope
+    return e;
+  }
+  cudaError_t put_items(int2 **d, int ntiles) {
+    std::vector<int2> h((size_t)ntiles);
+    for (int k = 0; k < ntiles; ++k) h[k] = make_int2(0, k);
+    cudaError_t e = alloc(d, (size_t)ntiles);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(*d, h.data(), sizeof(int2) * ntiles, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e;
+  }
+};
+
+int check_sets(const char *fn, int dim, int ni, int nj, int order, double width) {
+  if (dim != 2 && dim != 3) {
+    set_err("%s: dim must be 2 or 3", fn);
+    return LDDMM_ERR_ARG;
+  }
+  if (ni < 1 || nj < 1 || !(width > 0)) {
+    set_err("%s: empty point set or non-positive kernel width", fn);
+    return LDDMM_ERR_ARG;
+  }
+  if (order < -1 || order > 4) {
+    set_err("%s: kernel order %d not supported (Gaussian -1, Matern 0..4)", fn, order);
+    return LDDMM_ERR_UNSUPPORTED;
+  }
+  return 0;
+}
+
+// Calls f.template run<D, ORDER>() for the runtime (dim, order).
+template <class F>
+cudaError_t with_kernel(int dim, int order, F &f) {
+#define LDDMM_ORDERS(D)                                  \
+  switch (order) {                                       \
+    case -1: return f.template run<D, -1>();             \
+    case 0: return f.template run<D, 0>();               \
+    case 1: return f.template run<D, 1>();               \
+    case 2: return f.template run<D, 2>();               \
+    case 3: return f.template run<D, 3>();               \
+    case 4: return f.template run<D, 4>();               \
+  }
+  if (dim == 2) {
+    LDDMM_ORDERS(2)
+  } else {
+    LDDMM_ORDERS(3)
+  }
+#undef LDDMM_ORDERS
+  return cudaErrorInvalidValue;
+}
+
+// One cross sum: rows = set a (na points), columns = set b (nb_pad padded points).
+struct CrossRun {
+  cudaStream_t st;
+  int mode;
+  const float4 *qa, *xa, *qb, *yb;
+  int na, na_pad, nb_pad;
+  double fac;
+  double *out;
+  const int2 *items;
+  template <int D, int ORDER>
+  cudaError_t run() {
+    const int ntiles = na_pad / kTile;
+    if (mode == kCrossMul) {
+      CrossOp<D, ORDER, kCrossMul> op;
+      op.qa = qa; op.xa = xa; op.qb = qb; op.yb = yb;
+      op.na = na; op.nb_pad = nb_pad; op.fac = fac; op.out = out;
+      return launch_sweep(op, items, ntiles, default_cluster(ntiles), st);
+    }
+    CrossOp<D, ORDER, kCrossDq> op;
+    op.qa = qa; op.xa = xa; op.qb = qb; op.yb = yb;
+    op.na = na; op.nb_pad = nb_pad; op.fac = fac; op.out = out;
+    return launch_sweep(op, items, ntiles, default_cluster(ntiles), st);
+  }
+};
+
+struct MatrixRun {
+  cudaStream_t st;
+  const float4 *qi, *qj;
+  int ni, nj;
+  double *K;
+  template <int D, int ORDER>
+  cudaError_t run() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long total = (long long)ni * nj;
+    const long long want = (total + 255) / 256;
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(want, 8LL * sms));
+    return launch(kernel_matrix_kernel<D, ORDER>, grid, 256, 0, st, qi, ni, qj, nj, K);
+  }
+};
+
+}  // namespace
+
+extern "C" int lddmm_compute_kernel(int dim, int ni, const double *qi, int nj, const double *qj,
+                                    int order, double width, double *knl) {
+  if (!qj) nj = ni;
+  int rc = check_sets("lddmm_compute_kernel", dim, ni, nj, order, width);
+  if (rc) return rc;
+  if (!qi || !knl) {
+    set_err("lddmm_compute_kernel: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  if (!qj) qj = qi;
+  float kscale = 1.0f;
+  double pd_fac = 0.0;
+  def_kernel_scales(order, dim, width, &kscale, &pd_fac);
+  OneShot w;
+  CU(w.init());
+  float4 *dqi = nullptr, *dqj = nullptr;
+  double *dk = nullptr;
+  CU(w.put_points(&dqi, qi, ni, ni, dim, kscale));
+  CU(w.put_points(&dqj, qj, nj, nj, dim, kscale));
+  const size_t total = (size_t)ni * (size_t)nj;
+  CU(w.alloc(&dk, total));
+  MatrixRun m{w.st, dqi, dqj, ni, nj, dk};
+  CU(with_kernel(dim, order, m));
+  CU(cudaMemcpyAsync(knl, dk, sizeof(double) * total, cudaMemcpyDeviceToHost, w.st));
+  CU(cudaStreamSynchronize(w.st));
+  return 0;
+}
+
+extern "C" int lddmm_multiply_kernel2(int dim, int ni, const double *qi, int nj,
+                                      const double *qj, const double *a, int order,
+                                      double width, double *v) {
+  int rc = check_sets("lddmm_multiply_kernel2", dim, ni, nj, order, width);
+  if (rc) return rc;
+  if (!qi || !qj || !a || !v) {
+    set_err("lddmm_multiply_kernel2: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  float kscale = 1.0f;
+  double pd_fac = 0.0;
+  def_kernel_scales(order, dim, width, &kscale, &pd_fac);
+  const int ni_pad = pad_to(ni, kTile), nj_pad = pad_to(nj, kTile);
+  OneShot w;
+  CU(w.init());
+  float4 *dqi = nullptr, *dqj = nullptr, *da = nullptr;
+  int2 *items = nullptr;
+  double *dv = nullptr;
+  CU(w.put_points(&dqi, qi, ni, ni_pad, dim, kscale));
+  CU(w.put_points(&dqj, qj, nj, nj_pad, dim, kscale));
+  CU(w.put_points(&da, a, nj, nj_pad, dim, 1.0));
+  CU(w.put_items(&items, ni_pad / kTile));
+  CU(w.alloc(&dv, (size_t)ni * dim));
+  CrossRun r{w.st, kCrossMul, dqi, nullptr, dqj, da, ni, ni_pad, nj_pad, 1.0, dv, items};
+  CU(with_kernel(dim, order, r));
+  CU(cudaMemcpyAsync(v, dv, sizeof(double) * ni * dim, cudaMemcpyDeviceToHost, w.st));
+  CU(cudaStreamSynchronize(w.st));
+  return 0;
+}
+
+extern "C" int lddmm_dq_kernel2(int dim, int ni, const double *qi, int nj, const double *qj,
+                                const double *l, const double *r, int order, double width,
+                                double *dqi, double *dqj) {
+  int rc = check_sets("lddmm_dq_kernel2", dim, ni, nj, order, width);
+  if (rc) return rc;
+  if (!qi || !qj || !l || !r || !dqi || !dqj) {
+    set_err("lddmm_dq_kernel2: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  float kscale = 1.0f;
+  double pd_fac = 0.0;
+  def_kernel_scales(order, dim, width, &kscale, &pd_fac);
+  const int ni_pad = pad_to(ni, kTile), nj_pad = pad_to(nj, kTile);
+  OneShot w;
+  CU(w.init());
+  float4 *dqi_s = nullptr, *dqj_s = nullptr, *dl = nullptr, *dr = nullptr;
+  int2 *items_i = nullptr, *items_j = nullptr;
+  double *oi = nullptr, *oj = nullptr;
+  CU(w.put_points(&dqi_s, qi, ni, ni_pad, dim, kscale));
+  CU(w.put_points(&dqj_s, qj, nj, nj_pad, dim, kscale));
+  CU(w.put_points(&dl, l, ni, ni_pad, dim, 1.0));
+  CU(w.put_points(&dr, r, nj, nj_pad, dim, 1.0));
+  CU(w.put_items(&items_i, ni_pad / kTile));
+  CU(w.put_items(&items_j, nj_pad / kTile));
+  CU(w.alloc(&oi, (size_t)ni * dim));
+  CU(w.alloc(&oj, (size_t)nj * dim));
+  // i side: rows qi with l, columns qj with r; j side: rows qj with r, columns qi with l
+  CrossRun a{w.st, kCrossDq, dqi_s, dl, dqj_s, dr, ni, ni_pad, nj_pad, pd_fac, oi, items_i};
+  CU(with_kernel(dim, order, a));
+  CrossRun b{w.st, kCrossDq, dqj_s, dr, dqi_s, dl, nj, nj_pad, ni_pad, pd_fac, oj, items_j};
+  CU(with_kernel(dim, order, b));
+  CU(cudaMemcpyAsync(dqi, oi, sizeof(double) * ni * dim, cudaMemcpyDeviceToHost, w.st));
+  CU(cudaMemcpyAsync(dqj, oj, sizeof(double) * nj * dim, cudaMemcpyDeviceToHost, w.st));
+  CU(cudaStreamSynchronize(w.st));
   return 0;
 }
 

@@ -171,6 +171,72 @@ void orc_compute_kernel(double *K, const double *q, int order, double width, int
 			                               order, dim);
 }
 
+/* computeKernel.cpp:246-: two point sets, the reference's column-major ni x nj
+ * matrix, K[j * ni + i] = K(qi_i, qj_j). */
+void orc_compute_kernel2(double *K, const double *qi, int ni, const double *qj, int nj, int order,
+                         double width, int dim)
+{
+#pragma omp parallel for schedule(static)
+	for (int j = 0; j < nj; ++j)
+		for (int i = 0; i < ni; ++i)
+			K[(size_t)j * ni + i] = knl_val(dist(qi + (size_t)i * dim, qj + (size_t)j * dim, dim)
+			                                / width, order, dim);
+}
+
+/* multiplyKernel.cpp:294-: v_i = sum_j K(qi_i, qj_j) a_j (a given on the j set) */
+void orc_multiply_kernel2(double *v, const double *qi, int ni, const double *qj, int nj,
+                          const double *a, int order, double width, int dim)
+{
+#pragma omp parallel for schedule(static)
+	for (int i = 0; i < ni; ++i) {
+		double acc[3] = {0.0, 0.0, 0.0};
+		const double *x = qi + (size_t)i * dim;
+		for (int j = 0; j < nj; ++j) {
+			double k = knl_val(dist(x, qj + (size_t)j * dim, dim) / width, order, dim);
+			for (int d = 0; d < dim; ++d) acc[d] += k * a[(size_t)j * dim + d];
+		}
+		for (int d = 0; d < dim; ++d) v[(size_t)i * dim + d] = acc[d];
+	}
+}
+
+/* dqKernel.cpp:307-: l on the i set, r on the j set,
+ *   dqi_i = sum_j (l_i.r_j) c(d_ij) (qi_i - qj_j),  dqj_j = sum_i (l_i.r_j) c(d_ij) (qj_j - qi_i).
+ * Two independent passes (over i for dqi, over j for dqj). */
+void orc_dq_kernel2(double *dqi, double *dqj, const double *qi, int ni, const double *qj, int nj,
+                    const double *l, const double *r, int order, double width, int dim)
+{
+	double w2 = width * width;
+	int has_grad = (order == -1) || (order >= 1 && order <= 4);
+#pragma omp parallel for schedule(static)
+	for (int i = 0; i < ni; ++i) {
+		double acc[3] = {0.0, 0.0, 0.0};
+		const double *x = qi + (size_t)i * dim, *li = l + (size_t)i * dim;
+		if (has_grad) {
+			for (int j = 0; j < nj; ++j) {
+				const double *y = qj + (size_t)j * dim, *rj = r + (size_t)j * dim;
+				double c = knl_dq(dist(x, y, dim) / width, order, dim, w2), lr = 0.0;
+				for (int d = 0; d < dim; ++d) lr += li[d] * rj[d];
+				for (int d = 0; d < dim; ++d) acc[d] += lr * c * (x[d] - y[d]);
+			}
+		}
+		for (int d = 0; d < dim; ++d) dqi[(size_t)i * dim + d] = acc[d];
+	}
+#pragma omp parallel for schedule(static)
+	for (int j = 0; j < nj; ++j) {
+		double acc[3] = {0.0, 0.0, 0.0};
+		const double *y = qj + (size_t)j * dim, *rj = r + (size_t)j * dim;
+		if (has_grad) {
+			for (int i = 0; i < ni; ++i) {
+				const double *x = qi + (size_t)i * dim, *li = l + (size_t)i * dim;
+				double c = knl_dq(dist(x, y, dim) / width, order, dim, w2), lr = 0.0;
+				for (int d = 0; d < dim; ++d) lr += li[d] * rj[d];
+				for (int d = 0; d < dim; ++d) acc[d] += lr * c * (y[d] - x[d]);
+			}
+		}
+		for (int d = 0; d < dim; ++d) dqj[(size_t)j * dim + d] = acc[d];
+	}
+}
+
 /* dqKernel.cpp:31-305: dq_i = sum_j (l_i.r_j + l_j.r_i) c(d_ij) (q_i - q_j) */
 void orc_dq_kernel(double *dq, const double *q, const double *l, const double *r, int order,
                    double width, int n, int dim)

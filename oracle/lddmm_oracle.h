@@ -50,6 +50,12 @@ void orc_multiply_kernel(double *v, const double *q, const double *a, int order,
 void orc_dq_kernel(double *dq, const double *q, const double *l, const double *r, int order,
                    double width, int n, int dim);
 void orc_compute_kernel(double *K, const double *q, int order, double width, int n, int dim);
+void orc_compute_kernel2(double *K, const double *qi, int ni, const double *qj, int nj, int order,
+                         double width, int dim);
+void orc_multiply_kernel2(double *v, const double *qi, int ni, const double *qj, int nj,
+                          const double *a, int order, double width, int dim);
+void orc_dq_kernel2(double *dqi, double *dqj, const double *qi, int ni, const double *qj, int nj,
+                    const double *l, const double *r, int order, double width, int dim);
 
 int orc_varifold(const orc_problem *P, const double *nde, double *val, double *dq);
 /* Varifold value only, used to time the target self-term alone. */

@@ -131,6 +131,40 @@ class Oracle:
                                C.c_int(q.shape[0]), C.c_int(q.shape[1]))
         return dq
 
+    def compute_kernel(self, q, order, width):
+        """(n, n) matrix K(q_i, q_j) (computeKernel.cpp:21)."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        K = np.zeros((q.shape[0], q.shape[0]))
+        self.lib.orc_compute_kernel(_d(K), _d(q), C.c_int(order), C.c_double(width),
+                                    C.c_int(q.shape[0]), C.c_int(q.shape[1]))
+        return K
+
+    # two point sets (computeKernel.cpp:246, multiplyKernel.cpp:294, dqKernel.cpp:307)
+    def compute_kernel2(self, qi, qj, order, width):
+        """(ni, nj) matrix K(qi_i, qj_j)."""
+        qi, qj = (np.ascontiguousarray(x, dtype=np.float64) for x in (qi, qj))
+        K = np.zeros((qj.shape[0], qi.shape[0]))  # column-major ni x nj
+        self.lib.orc_compute_kernel2(_d(K), _d(qi), C.c_int(qi.shape[0]), _d(qj),
+                                     C.c_int(qj.shape[0]), C.c_int(order), C.c_double(width),
+                                     C.c_int(qi.shape[1]))
+        return K.T.copy()
+
+    def multiply_kernel2(self, qi, qj, a, order, width):
+        qi, qj, a = (np.ascontiguousarray(x, dtype=np.float64) for x in (qi, qj, a))
+        v = np.zeros_like(qi)
+        self.lib.orc_multiply_kernel2(_d(v), _d(qi), C.c_int(qi.shape[0]), _d(qj),
+                                      C.c_int(qj.shape[0]), _d(a), C.c_int(order),
+                                      C.c_double(width), C.c_int(qi.shape[1]))
+        return v
+
+    def dq_kernel2(self, qi, qj, l, r, order, width):
+        qi, qj, l, r = (np.ascontiguousarray(x, dtype=np.float64) for x in (qi, qj, l, r))
+        dqi, dqj = np.zeros_like(qi), np.zeros_like(qj)
+        self.lib.orc_dq_kernel2(_d(dqi), _d(dqj), _d(qi), C.c_int(qi.shape[0]), _d(qj),
+                                C.c_int(qj.shape[0]), _d(l), _d(r), C.c_int(order),
+                                C.c_double(width), C.c_int(qi.shape[1]))
+        return dqi, dqj
+
     def elm_ifo(self, elm_vtx, nde_num):
         ev = np.ascontiguousarray(elm_vtx, dtype=np.int32)
         rows = self.lib.orc_elm_ifo(_i(ev), C.c_int(ev.shape[1]), C.c_int(ev.shape[0]),
@@ -235,6 +269,37 @@ class Reference:
         self.lib.ref_dq_kernel(_d(dq), _d(q), _d(l), _d(r), C.c_int(order), C.c_double(width),
                                C.c_int(q.shape[0]), C.c_int(q.shape[1]))
         return dq
+
+    def compute_kernel(self, q, order, width):
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        K = np.zeros((q.shape[0], q.shape[0]))  # column-major n x n
+        self.lib.ref_compute_kernel(_d(K), _d(q), C.c_int(order), C.c_double(width),
+                                    C.c_int(q.shape[0]), C.c_int(q.shape[1]))
+        return K.T.copy()
+
+    def compute_kernel2(self, qi, qj, order, width):
+        qi, qj = (np.ascontiguousarray(x, dtype=np.float64) for x in (qi, qj))
+        K = np.zeros((qj.shape[0], qi.shape[0]))
+        self.lib.ref_compute_kernel2(_d(K), _d(qi), C.c_int(qi.shape[0]), _d(qj),
+                                     C.c_int(qj.shape[0]), C.c_int(order), C.c_double(width),
+                                     C.c_int(qi.shape[1]))
+        return K.T.copy()
+
+    def multiply_kernel2(self, qi, qj, a, order, width):
+        qi, qj, a = (np.ascontiguousarray(x, dtype=np.float64) for x in (qi, qj, a))
+        v = np.zeros_like(qi)
+        self.lib.ref_multiply_kernel2(_d(v), _d(qi), C.c_int(qi.shape[0]), _d(qj),
+                                      C.c_int(qj.shape[0]), _d(a), C.c_int(order),
+                                      C.c_double(width), C.c_int(qi.shape[1]))
+        return v
+
+    def dq_kernel2(self, qi, qj, l, r, order, width):
+        qi, qj, l, r = (np.ascontiguousarray(x, dtype=np.float64) for x in (qi, qj, l, r))
+        dqi, dqj = np.zeros_like(qi), np.zeros_like(qj)
+        self.lib.ref_dq_kernel2(_d(dqi), _d(dqj), _d(qi), C.c_int(qi.shape[0]), _d(qj),
+                                C.c_int(qj.shape[0]), _d(l), _d(r), C.c_int(order),
+                                C.c_double(width), C.c_int(qi.shape[1]))
+        return dqi, dqj
 
 
 class ReferenceCuda:

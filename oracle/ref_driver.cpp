@@ -32,6 +32,10 @@ void varifoldITF(double *, double *, double *, fcndata &);
 void computeKernel(double *, double *, int, double, int, int);
 void multiplyKernel(double *, double *, double *, int, double, int, int);
 void dqKernel(double *, double *, double *, double *, int, double, int, int);
+void computeKernel(double *, double *, double *, int, double, int, int, int);
+void multiplyKernel(double *, double *, double *, double *, int, double, int, int, int);
+void dqKernel(double *, double *, double *, double *, double *, double *, int, double, int, int,
+              int);
 
 static std::vector<double> g_trace_f;
 static std::vector<double> g_trace_g2;
@@ -198,6 +202,32 @@ void ref_compute_kernel(double *K, const double *q, int order, double width, int
 {
 	std::vector<double> qq(q, q + (size_t)dim * n);
 	computeKernel(K, qq.data(), order, width, n, dim);
+}
+
+/* Two-set overloads (computeKernel.cpp:246, multiplyKernel.cpp:294, dqKernel.cpp:307):
+ * K[j * ni + i] = K(qi_i, qj_j); v_i = sum_j K(qi_i, qj_j) a_j;
+ * dqi_i = sum_j (l_i . r_j) c (qi_i - qj_j), dqj_j = sum_i (l_i . r_j) c (qj_j - qi_i). */
+void ref_compute_kernel2(double *K, const double *qi, int ni, const double *qj, int nj, int order,
+                         double width, int dim)
+{
+	std::vector<double> a(qi, qi + (size_t)dim * ni), b(qj, qj + (size_t)dim * nj);
+	computeKernel(K, a.data(), b.data(), order, width, ni, nj, dim);
+}
+
+void ref_multiply_kernel2(double *v, const double *qi, int ni, const double *qj, int nj,
+                          const double *a, int order, double width, int dim)
+{
+	std::vector<double> x(qi, qi + (size_t)dim * ni), y(qj, qj + (size_t)dim * nj),
+	    aa(a, a + (size_t)dim * nj);
+	multiplyKernel(v, x.data(), y.data(), aa.data(), order, width, ni, nj, dim);
+}
+
+void ref_dq_kernel2(double *dqi, double *dqj, const double *qi, int ni, const double *qj, int nj,
+                    const double *l, const double *r, int order, double width, int dim)
+{
+	std::vector<double> x(qi, qi + (size_t)dim * ni), y(qj, qj + (size_t)dim * nj),
+	    ll(l, l + (size_t)dim * ni), rr(r, r + (size_t)dim * nj);
+	dqKernel(dqi, dqj, x.data(), y.data(), ll.data(), rr.data(), order, width, ni, nj, dim);
 }
 
 } /* extern "C" */

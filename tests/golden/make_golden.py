@@ -58,6 +58,29 @@ def kernels(dim, seed):
     save(f"kernels_{dim}d", **arrays)
 
 
+def two_set_kernels(dim, seed):
+    """The two-point-set overloads (computeKernel.cpp:246, multiplyKernel.cpp:294,
+    dqKernel.cpp:307) and the one-set kernel matrix (computeKernel.cpp:21)."""
+    R = Reference(dim)
+    rng = np.random.default_rng(seed)
+    ni, nj = 48, 37
+    qi = rng.uniform(-1, 1, size=(ni, dim))
+    qj = rng.uniform(-1, 1, size=(nj, dim))
+    a = rng.normal(size=(nj, dim))
+    l = rng.normal(size=(ni, dim))
+    r = rng.normal(size=(nj, dim))
+    arrays = dict(qi=qi, qj=qj, a=a, l=l, r=r, width=np.array(0.5))
+    for order in (-1, 0, 1, 2, 3, 4):
+        tag = f"m{order}" if order >= 0 else "g"
+        arrays[f"K_{tag}"] = R.compute_kernel2(qi, qj, order, 0.5)
+        arrays[f"K1_{tag}"] = R.compute_kernel(qi, order, 0.5)
+        arrays[f"v_{tag}"] = R.multiply_kernel2(qi, qj, a, order, 0.5)
+        dqi, dqj = R.dq_kernel2(qi, qj, l, r, order, 0.5)
+        arrays[f"dqi_{tag}"] = dqi
+        arrays[f"dqj_{tag}"] = dqj
+    save(f"two_set_kernels_{dim}d", **arrays)
+
+
 def sphere2cube_example():
     import scipy.io as sio
     ex = os.path.join(REF_TREE, "Cpp", "examples", "sphere2cube")
@@ -174,6 +197,8 @@ def objgrd_orders_2d():
 if __name__ == "__main__":
     kernels(2, 1)
     kernels(3, 2)
+    two_set_kernels(2, 11)
+    two_set_kernels(3, 12)
     circle2square()
     circle2square_example()
     sphere2cube_example()

@@ -172,9 +172,10 @@ def reference_workers() -> int:
 def run_reference(args):
     import multiprocessing as mp
 
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
+    from lddmm_b200 import replicas
+
+    if not replicas.rank_env().reports:
+        return  # the reference arm runs on rank 0 alone; the other ranks exit
     n = reference_workers()
     ctx = mp.get_context("spawn")
     with ctx.Pool(n) as pool:
@@ -216,19 +217,12 @@ def run_ours(args):
     import numpy as np
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from lddmm_b200 import _lib, api, replicas
+
+    env = replicas.rank_env()
+    world, rank, local = env.world, env.rank, env.local
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    from lddmm_b200 import _lib, api
+    dist = replicas.init(env, "nccl")
 
     P = workload()
     # one explicit stream shared by torch and the context, so that the CUDA events
@@ -254,8 +248,7 @@ def run_ours(args):
         flush.zero_()
         registration()
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     torch.cuda.synchronize()
     launches = 0
     evals = 0
@@ -271,11 +264,8 @@ def run_ours(args):
         t_end.record(stream)
         torch.cuda.synchronize()
     ms = t_start.elapsed_time(t_end)
-    if dist:
-        dist.barrier()
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    replicas.barrier(dist)
+    ms = replicas.max_over_ranks(dist, ms, "cuda")  # the job lasts as long as its slowest rank
     clocks = clk.summary()
     r = res[0]
     x = d_alp.cpu().numpy()
@@ -299,8 +289,7 @@ def run_ours(args):
 
     e2e_call()
     torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    replicas.barrier(dist)
     e_steps = max(1, min(args.steps, 3))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -309,11 +298,7 @@ def run_ours(args):
         _lib.check(min(e2e_call(), 0))
     e1.record(stream)
     torch.cuda.synchronize()
-    e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e_ms = float(t.item())
+    e_ms = replicas.max_over_ranks(dist, e0.elapsed_time(e1), "cuda")
     h2d = (ini.nbytes + alp0.nbytes + P.elm_vtx.nbytes + ifo.nbytes + P.tgt_cen.nbytes
            + P.tgt_dir.nbytes + P.tgt_vol.nbytes)
     d2h = out.nbytes
@@ -368,8 +353,7 @@ def run_ours(args):
 
     pairs_per_eval = 2 * T * N * N + Ed * (Ed + Et)
     evals_per_reg = evals / max(args.steps, 1)
-    regs = args.steps * world
-    value = regs / (ms * 1e-3)
+    value = replicas.job_rate(args.steps, world, ms * 1e-3)
     gpairs = (evals * pairs_per_eval + args.steps * Et * Et) * world / (ms * 1e-3) / 1e9
 
     # accuracy at the returned point against the FP64 oracle (rank 0)
@@ -420,7 +404,7 @@ def run_ours(args):
                          "flops_per_pair": fl[dom], "pairs_per_launch": pairs_launch[dom],
                          "traffic": traffic},
             "cpu_baseline": cpu,
-            "e2e": {"value": e_steps / (e_ms * 1e-3) * world, "unit": UNIT,
+            "e2e": {"value": replicas.job_rate(e_steps, world, e_ms * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "call": "lddmm_LDDMM (host buffers; context set-up inside)"},
             "gpu_launches": launches,
@@ -429,9 +413,8 @@ def run_ours(args):
         }
         print(json.dumps(line), flush=True)
     ctx.close()
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.barrier(dist)
+    replicas.finish(dist)
 
 
 def run_objgrd(args):

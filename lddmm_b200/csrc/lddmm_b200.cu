@@ -278,7 +278,10 @@ static cudaError_t shoot_impl(lddmm_ctx &c, int t, double *vlc) {
   op.vlc64 = vlc;
   op.tile_part = c.reg_part + (size_t)t * c.ntile_tot;
   op.t = t;
-  return launch_sweep(op, c.pt_items, c.n_pt_items, c.S_shoot, c.stream);
+  // packed FP32x2 form of the same sweep (bitwise the same sums)
+  return launch(sweep_packed_kernel<ShootOp<D, ORDER>, kWarps>,
+                (unsigned)(c.n_pt_items * c.S_shoot), kWarps * 32, c.S_shoot, c.stream, op,
+                (const int2 *)c.pt_items, c.S_shoot);
 }
 
 template <int D, int ORDER>
@@ -297,7 +300,10 @@ static cudaError_t adjoint_impl(lddmm_ctx &c, int t, double *g, double *pdot) {
   op.ls_n = (t > 0) ? c.ls + (size_t)((t - 1) & 1) * c.NPtot : nullptr;
   op.pdot64 = pdot;
   op.t = t;
-  return launch_sweep(op, c.pt_items, c.n_pt_items, c.S_adj, c.stream);
+  // packed FP32x2 form of the same sweep (bitwise the same sums)
+  return launch(sweep_packed_kernel<AdjointOp<D, ORDER>, kWarps>,
+                (unsigned)(c.n_pt_items * c.S_adj), kWarps * 32, c.S_adj, c.stream, op,
+                (const int2 *)c.pt_items, c.S_adj);
 }
 
 // Cooperative launch of a persistent multi-step sweep (all CTAs co-resident; the

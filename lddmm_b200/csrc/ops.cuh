@@ -83,6 +83,63 @@ struct ShootOp {
     acc[1] = fmaf(K, w[1].y, acc[1]);
     if (D == 3) acc[D - 1] = fmaf(K, w[1].z, acc[D - 1]);
   }
+  // ---- packed form (sweep_packed_kernel): a lane's two rows in one FP32x2 operation,
+  // bitwise the scalar pair() per row (x - y == x + (-y); the scalar nr2, built with
+  // fma(-d, d, .), is exactly -(the sum of fma(d, d, .))).  Staged j point, each value
+  // twice: (-qx,-qx,-qy,-qy) (-qz,-qz,ax,ax) (ay,ay,az,az); 2D: (-qx,-qx,-qy,-qy)
+  // (ax,ax,ay,ay).
+  static constexpr bool kPacked = true;
+  static constexpr int JWP = (D == 3) ? 3 : 2;
+  struct IData2 {
+    float2 q[D];  // (row0, row1)
+  };
+  __device__ void load_i2(int p, int r0, int r1, IData2 &I) const {
+    IData a, b;
+    load_i(p, r0, a);
+    load_i(p, r1, b);
+    I.q[0] = make_float2(a.x, b.x);
+    I.q[1] = make_float2(a.y, b.y);
+    if (D == 3) I.q[D - 1] = make_float2(a.z, b.z);
+  }
+  __device__ void load_j2(int p, int j, float4 (&w)[JWP]) const {
+    float4 v[JW];
+    load_j(p, j, v);
+    if (D == 3) {
+      w[0] = make_float4(-v[0].x, -v[0].x, -v[0].y, -v[0].y);
+      w[1] = make_float4(-v[0].z, -v[0].z, v[1].x, v[1].x);
+      w[JWP - 1] = make_float4(v[1].y, v[1].y, v[1].z, v[1].z);
+    } else {
+      w[0] = make_float4(-v[0].x, -v[0].x, -v[0].y, -v[0].y);
+      w[1] = make_float4(v[1].x, v[1].x, v[1].y, v[1].y);
+    }
+  }
+  template <int SET>
+  __device__ __forceinline__ void pair2(const IData2 &I, const float4 (&w)[JWP],
+                                        float2 (&acc)[NA]) const {
+    float2 mq[D], aj[D];
+    mq[0] = make_float2(w[0].x, w[0].y);
+    mq[1] = make_float2(w[0].z, w[0].w);
+    if (D == 3) {
+      mq[D - 1] = make_float2(w[1].x, w[1].y);
+      aj[0] = make_float2(w[1].z, w[1].w);
+      aj[1] = make_float2(w[JWP - 1].x, w[JWP - 1].y);
+      aj[D - 1] = make_float2(w[JWP - 1].z, w[JWP - 1].w);
+    } else {
+      aj[0] = make_float2(w[1].x, w[1].y);
+      aj[1] = make_float2(w[1].z, w[1].w);
+    }
+    const float2 dx = __fadd2_rn(I.q[0], mq[0]);
+    float2 r2 = __fmul2_rn(dx, dx);
+#pragma unroll
+    for (int d = 1; d < D; ++d) {
+      const float2 dd = __fadd2_rn(I.q[d], mq[d]);
+      r2 = __ffma2_rn(dd, dd, r2);
+    }
+    const float2 K = make_float2(DefKernelOf<D, ORDER>::type::val(-r2.x),
+                                 DefKernelOf<D, ORDER>::type::val(-r2.y));
+#pragma unroll
+    for (int d = 0; d < D; ++d) acc[d] = __ffma2_rn(K, aj[d], acc[d]);
+  }
   // finalize operands (loaded before the row sums are complete): q_t and a_t of the row
   struct FData {
     double q[3], a[3];
@@ -231,6 +288,79 @@ struct AdjointOp {
     for (int d = 0; d < D; ++d) {
       acc[d] = fmaf(K, uj[d], acc[d]);
       acc[D + d] = fmaf(s, dq[d], acc[D + d]);
+    }
+  }
+  // ---- packed form (sweep_packed_kernel): a lane's two rows in one FP32x2 operation,
+  // bitwise the scalar pair() per row (same operations in the same order; x - y is
+  // computed as x + (-y), and nr2 as -(the sum of fma(d, d, .))).  Staged j point,
+  // each value twice: -q, u, l, r (3D: 6 float4, 2D: 4).
+  static constexpr bool kPacked = true;
+  static constexpr int JWP = (D == 3) ? 6 : 4;
+  struct IData2 {
+    float2 q[D], l[D], r[D];  // (row0, row1)
+  };
+  __device__ void load_i2(int p, int r0, int r1, IData2 &I) const {
+    IData a, b;
+    load_i(p, r0, a);
+    load_i(p, r1, b);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      I.q[d] = make_float2(a.q[d], b.q[d]);
+      I.l[d] = make_float2(a.l[d], b.l[d]);
+      I.r[d] = make_float2(a.r[d], b.r[d]);
+    }
+  }
+  __device__ void load_j2(int p, int j, float4 (&w)[JWP]) const {
+    const int g = pd[p].pt_off + j;
+    const float4 q = __ldcg(&qs_t[g]), u = __ldcg(&us_t[g]), l = __ldcg(&ls_t[g]),
+                 r = __ldcg(&as_t[g]);
+    // value k of the 4D-padded list (-q, u, l, r) sits at float pair k of w
+    float v[4 * D];
+    const float qq[3] = {q.x, q.y, q.z}, uu[3] = {u.x, u.y, u.z}, ll[3] = {l.x, l.y, l.z},
+                rr[3] = {r.x, r.y, r.z};
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      v[d] = -qq[d];
+      v[D + d] = uu[d];
+      v[2 * D + d] = ll[d];
+      v[3 * D + d] = rr[d];
+    }
+#pragma unroll
+    for (int k = 0; k < JWP; ++k)
+      w[k] = make_float4(v[2 * k], v[2 * k], v[2 * k + 1], v[2 * k + 1]);
+  }
+  template <int SET>
+  __device__ __forceinline__ void pair2(const IData2 &I, const float4 (&w)[JWP],
+                                        float2 (&acc)[NA]) const {
+    float2 v[4 * D];
+#pragma unroll
+    for (int k = 0; k < JWP; ++k) {
+      v[2 * k] = make_float2(w[k].x, w[k].y);
+      v[2 * k + 1] = make_float2(w[k].z, w[k].w);
+    }
+    const float2 *mq = v, *uj = v + D, *lj = v + 2 * D, *rj = v + 3 * D;
+    float2 dq[D];
+    dq[0] = __fadd2_rn(I.q[0], mq[0]);
+    float2 r2 = __fmul2_rn(dq[0], dq[0]);
+#pragma unroll
+    for (int d = 1; d < D; ++d) {
+      dq[d] = __fadd2_rn(I.q[d], mq[d]);
+      r2 = __ffma2_rn(dq[d], dq[d], r2);
+    }
+    float Kx, Wx, Ky, Wy;
+    DefKernelOf<D, ORDER>::type::val_w(-r2.x, Kx, Wx);
+    DefKernelOf<D, ORDER>::type::val_w(-r2.y, Ky, Wy);
+    const float2 K = make_float2(Kx, Ky), Wt = make_float2(Wx, Wy);
+    float2 lr = __fmul2_rn(I.l[0], rj[0]);
+#pragma unroll
+    for (int d = 1; d < D; ++d) lr = __ffma2_rn(I.l[d], rj[d], lr);
+#pragma unroll
+    for (int d = 0; d < D; ++d) lr = __ffma2_rn(lj[d], I.r[d], lr);
+    const float2 sv = __fmul2_rn(lr, Wt);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      acc[d] = __ffma2_rn(K, uj[d], acc[d]);
+      acc[D + d] = __ffma2_rn(sv, dq[d], acc[D + d]);
     }
   }
   // finalize operands loaded before the row sums are complete: p of the row and, when

@@ -94,6 +94,32 @@ def test_lbfgs_batch_equals_individual(api):
         assert np.array_equal(xs[k], x1)
 
 
+def test_lbfgs_nonfinite_pair_fails_alone(api):
+    """A pair whose starting objective is not finite stops with LDDMM_ERR_NONFINITE
+    (-3); the other pairs of the batch run exactly as they would alone, and the call
+    returns the first non-zero pair status, as LBFGS.cpp:92 reports a failure."""
+    import ctypes as C
+
+    from lddmm_b200 import _lib, problem
+
+    probs = [problem.circle_to_square(n_src=n, n_tgt=64, time_num=6) for n in (40, 100)]
+    shape = dict(cluster=(1, 1, 1), persistent=-1)
+    with api.Context(probs, **shape) as ctx:
+        x = np.zeros(ctx.var_total)
+        x[0] = np.nan  # first variable of pair 0
+        opt = _lib.Opt(25, 1e-6, 1e-4, 0.9, 5, 0, 0.0)
+        res = (_lib.Result * 2)()
+        rc = _lib.lib.lddmm_lbfgs(ctx.handle, C.byref(opt), _lib.dptr(x), res)
+        xs = ctx.split(x)
+    assert rc == -3
+    assert res[0].status == -3 and res[0].iters == 0
+    assert res[1].status == 0
+    with api.Context(probs[1], **shape) as c1:
+        x1, r1 = c1.lbfgs(np.zeros(probs[1].var_num), itr_max=25)
+    assert res[1].iters == r1[0]["iters"] and res[1].fcn == r1[0]["f"]
+    assert np.array_equal(xs[1], x1)
+
+
 def test_lbfgs_graph_and_direct_launches_agree(api):
     from lddmm_b200 import problem
 

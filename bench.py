@@ -57,12 +57,13 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--itr", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["registration", "objgrd", "large_pair"],
+    ap.add_argument("--mode", choices=["registration", "objgrd", "large_pair", "ws_gemm"],
                     default="registration",
                     help="objgrd: only time device-resident objective+gradient evaluations "
                          "(the command the ncu captures in profiles/ use); large_pair: the "
                          "163,842-landmark star-surface pair, --itr L-BFGS iterations "
-                         "timed (default 100)")
+                         "timed (default 100); ws_gemm: the warm-start network's tcgen05 "
+                         "BF16 GEMM on its layer shapes, against the bf16 peak and torch")
     ap.add_argument("--evals", type=int, default=20)
     ap.add_argument("--subdiv", type=int, default=4,
                     help="objgrd mode: icosphere subdivisions of the source (4: 2562 points)")
@@ -510,8 +511,78 @@ def run_large_pair(args):
     ctx.close()
 
 
+def _bf16_peak():
+    """Dense bf16 TFLOP/s: the pool's measured figure when the file is present, else
+    the earlier measurement on this pool (burst)."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["bf16_tflops"]), "measured (MEASURED_PEAKS.json, burst)"
+    except (OSError, ValueError, KeyError, TypeError):
+        return 1590.0, "fallback 1.59 PFLOP/s (earlier measurement on this pool)"
+
+
+def run_ws_gemm(args):
+    """C[m x n] = A[m x k] B[n x k]^T in BF16 with FP32 output through
+    lddmm_ws_gemm_bf16 (tcgen05.mma, TMEM accumulator), on the warm-start network's
+    layer shapes at a 64-pair batch (2562 points or 5120 triangles per pair), CUDA
+    events around each launch with a 256 MiB L2 flush before it; torch's bf16 matmul
+    (cuBLAS) on the same shapes for context.  Prints one JSON line."""
+    import ctypes as C
+
+    import torch
+
+    from lddmm_b200 import _lib
+
+    torch.cuda.set_device(0)
+    peak, peak_src = _bf16_peak()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    shapes = [(64 * 2562, 256, 256), (64 * 2562, 256, 80), (64 * 2562, 32, 256),
+              (64 * 5120, 64, 64), (64 * 2562, 256, 2048)]
+    out = []
+    for m, n, k in shapes:
+        a = torch.randn(m, k, device="cuda").to(torch.bfloat16)
+        b = torch.randn(n, k, device="cuda").to(torch.bfloat16)
+        c = torch.empty(m, n, device="cuda", dtype=torch.float32)
+
+        def ours():
+            _lib.check(_lib.lib.lddmm_ws_gemm_bf16(
+                C.c_void_p(a.data_ptr()), k, C.c_void_p(b.data_ptr()), k, m, n, k,
+                C.c_void_p(c.data_ptr()), n, C.c_void_p(stream.cuda_stream)))
+
+        def ref():
+            torch.matmul(a, b.t())
+
+        res = {}
+        for name, fn in (("ours", ours), ("torch", ref)):
+            for _ in range(max(args.warmup, 3)):
+                fn()
+            ts = []
+            for _ in range(max(args.steps, 5)):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            ms = statistics.median(ts)
+            res[name] = {"ms": ms, "tflops": 2.0 * m * n * k / (ms * 1e-3) / 1e12}
+        err = float((c - torch.matmul(a.float(), b.float().t())).abs().max()
+                    / torch.matmul(a.float(), b.float().t()).abs().max())
+        out.append({"m": m, "n": n, "k": k, "ours": res["ours"], "torch_bf16": res["torch"],
+                    "frac_of_peak": res["ours"]["tflops"] / peak, "rel_err_vs_fp32": err})
+    print(json.dumps({"mode": "ws_gemm", "peak_tflops": peak, "peak_source": peak_src,
+                      "shapes": out}), flush=True)
+
+
 def main():
     args = parse()
+    if args.mode == "ws_gemm":
+        run_ws_gemm(args)
+        return
     if args.mode == "objgrd":
         run_objgrd(args)
         return

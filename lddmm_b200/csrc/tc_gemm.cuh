@@ -9,10 +9,14 @@
 // K-major layout without swizzle: "core matrices" of 8 rows x 16 bytes, core (g, c)
 // (row group g, 8-element K group c) at byte (g * kKC / 8 + c) * 128, so the leading
 // byte offset (next K group) is 128 and the stride byte offset (next row group) is
-// kKC * 16.  Thread 0 issues the MMAs of a chunk and commits them to an mbarrier; the
-// CTA waits on it (bounded) before restaging.  The epilogue reads the accumulator
-// with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = rows of the tile) and applies
-// bias / GELU / GELU' and writes FP32, BF16 and transposed BF16 outputs as asked.
+// kKC * 16.  Two stage buffers: while the MMAs of chunk i run, the CTA copies chunk
+// i + 1 into the other buffer with cp.async (global -> shared without registers);
+// thread 0 issues a chunk's MMAs and commits them to that buffer's mbarrier, and a
+// buffer is restaged only after its mbarrier (bounded wait) says the MMAs reading it
+// are done.  The epilogue reads the accumulator with tcgen05.ld (warp w owns TMEM
+// lanes 32w..32w+31 = rows of the tile), applies bias / GELU / GELU' and writes FP32,
+// BF16 and transposed BF16 outputs as asked, four columns per store where the
+// outputs are 16-byte (BF16: 8-byte) aligned.
 //
 // Shared-memory and instruction descriptor bit layouts follow the PTX ISA
 // (tcgen05 "Shared memory descriptor", "Instruction descriptor" for kind::f16).
@@ -137,29 +141,39 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 }
 
 // Stage rows [r0, r0 + rows) x K elements [k0, k0 + kKC) of a K-major matrix into the
-// canonical layout at `dst` (rows beyond `rmax` and K beyond `kmax` read as zero).
-__device__ __forceinline__ void stage(unsigned char *dst, const __nv_bfloat16 *src, long long ld,
-                                      int r0, int rows, int rmax, int k0, int kmax) {
+// canonical layout at `dst` with 16-byte cp.async copies (rows beyond `rmax` and K
+// beyond `kmax` are zero-filled: source size 0, source address clamped to `src`).
+// Callers guarantee 16-byte alignment: ld a multiple of 8 elements, k0 a multiple of 8.
+__device__ __forceinline__ void stage_async(unsigned char *dst, const __nv_bfloat16 *src,
+                                            long long ld, int r0, int rows, int rmax, int k0,
+                                            int kmax) {
   constexpr int kChunks = kKC / 8;  // 16-byte groups per row
   for (int i = threadIdx.x; i < rows * kChunks; i += kGemmThreads) {
     const int r = i / kChunks, c = i - r * kChunks;
     const int gr = r0 + r, gk = k0 + c * 8;
-    uint4 v = make_uint4(0u, 0u, 0u, 0u);
-    if (gr < rmax && gk < kmax) v = *reinterpret_cast<const uint4 *>(src + gr * ld + gk);
-    *reinterpret_cast<uint4 *>(dst + ((r >> 3) * kChunks + c) * 128 + (r & 7) * 16) = v;
+    const bool ok = gr < rmax && gk < kmax;
+    const __nv_bfloat16 *g = ok ? src + (long long)gr * ld + gk : src;
+    const uint32_t d = smem_u32(dst + ((r >> 3) * kChunks + c) * 128 + (r & 7) * 16);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(g),
+                 "r"(ok ? 16 : 0)
+                 : "memory");
   }
 }
 
 __global__ void __launch_bounds__(kGemmThreads, 1) gemm_bf16_kernel(GemmArgs g) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char *sA = smem;                                // kTileM x kKC bf16
-  unsigned char *sB = smem + kTileM * kKC * 2;             // N x kKC bf16
-  __shared__ uint64_t s_mbar;
+  const size_t stage_bytes = (size_t)(kTileM + g.N) * kKC * 2;
+  // stage buffer b: A tile (kTileM x kKC bf16) at smem + b * stage_bytes, B tile
+  // (N x kKC bf16) right after it
+  auto sA = [&](int b) { return smem + (size_t)b * stage_bytes; };
+  auto sB = [&](int b) { return smem + (size_t)b * stage_bytes + kTileM * kKC * 2; };
+  __shared__ uint64_t s_mbar[2];
   __shared__ uint32_t s_tmem;
   __shared__ int s_ok;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * kTileM;
   const int kb = blockIdx.y * g.k_split, ke = min(g.K, kb + g.k_split);
+  const int nk = ke > kb ? (ke - kb + kKC - 1) / kKC : 0;
   const uint32_t ncols = g.N <= 32 ? 32u : g.N <= 64 ? 64u : g.N <= 128 ? 128u : 256u;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -168,7 +182,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_bf16_kernel(GemmArgs g) 
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (threadIdx.x == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar)));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[0])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[1])));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_ok = 1;
   }
@@ -177,60 +192,130 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_bf16_kernel(GemmArgs g) 
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
   const uint32_t idesc = instr_desc_bf16(kTileM, g.N);
-  uint32_t phase = 0;
-  bool first = true;
-  for (int k0 = kb; k0 < ke; k0 += kKC) {
-    stage(sA, g.A, g.lda, m0, kTileM, g.M, k0, ke);
-    stage(sB, g.B, g.ldb, 0, g.N, g.N, k0, ke);
+  // MMA chunk j committed to s_mbar[j & 1]; each commit is waited exactly once, in
+  // order per barrier, with parity (j >> 1) & 1
+  auto wait_mma = [&](int j) {
+    if (!mbar_wait(&s_mbar[j & 1], (uint32_t)((j >> 1) & 1))) {
+      s_ok = 0;
+      if (g.error) atomicExch(g.error, 1u);
+    }
+  };
+  auto issue = [&](int buf, int k0) {
+    stage_async(sA(buf), g.A, g.lda, m0, kTileM, g.M, k0, ke);
+    stage_async(sB(buf), g.B, g.ldb, 0, g.N, g.N, k0, ke);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  if (nk > 0) issue(0, kb);
+  int done = -1;   // last MMA chunk waited for
+  int issued = 0;  // MMA chunks committed
+  for (int i = 0; i < nk; ++i) {
+    if (i + 1 < nk) {
+      // the other buffer was read by chunk i - 1: wait for its MMAs, then refill it
+      if (i >= 1) {
+        wait_mma(i - 1);
+        done = i - 1;
+        __syncthreads();
+        if (!s_ok) break;
+      }
+      issue((i + 1) & 1, kb + (i + 1) * kKC);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");  // chunk i has landed
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
     if (threadIdx.x == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+      const uint32_t a0 = smem_u32(sA(i & 1)), b0 = smem_u32(sB(i & 1));
 #pragma unroll
       for (int s = 0; s < kKC / 16; ++s) {
         // K step s covers K groups 2s and 2s + 1 (start advances by 2 core matrices)
         const uint64_t da = smem_desc(a0 + s * 256, 128, kKC * 16);
         const uint64_t db = smem_desc(b0 + s * 256, 128, kKC * 16);
-        mma_bf16(tmem, da, db, idesc, (first && s == 0) ? 0u : 1u);
+        mma_bf16(tmem, da, db, idesc, (i == 0 && s == 0) ? 0u : 1u);
       }
-      mma_commit(&s_mbar);
+      mma_commit(&s_mbar[i & 1]);
     }
-    first = false;
-    // every thread waits for the chunk's MMAs before the stage buffers are rewritten
-    if (!mbar_wait(&s_mbar, phase)) {
-      s_ok = 0;
-      if (g.error) atomicExch(g.error, 1u);
-    }
-    phase ^= 1u;
-    __syncthreads();
-    if (!s_ok) break;
+    ++issued;
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  // the remaining commits, oldest first
+  for (int j = done + 1; j < issued; ++j) wait_mma(j);
+  __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (s_ok && !first) {
+  if (s_ok && issued > 0) {
     const int m = m0 + warp * 32 + lane;
     const bool row_ok = m < g.M;
     float *out = g.out ? g.out + (size_t)blockIdx.y * g.split_stride : nullptr;
+    // four columns per store where every output in use allows it
+    const bool vec =
+        (!out || (((uintptr_t)out & 15u) == 0 && (g.ldo & 3) == 0)) &&
+        (!g.pre_out || (((uintptr_t)g.pre_out & 15u) == 0 && (g.ld_pre_out & 3) == 0)) &&
+        (!g.out_bf || (((uintptr_t)g.out_bf & 7u) == 0 && (g.ldb_out & 3) == 0)) &&
+        (g.epi != kEpiDGelu ||
+         (((uintptr_t)g.pre_in & 15u) == 0 && (g.ld_pre_in & 3) == 0));
     for (int c0 = 0; c0 < g.N; c0 += 32) {
       float v[32];
       tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
       if (!row_ok) continue;
-#pragma unroll 4
-      for (int j = 0; j < 32; ++j) {
+#pragma unroll
+      for (int j = 0; j < 32; j += 4) {
         const int n = c0 + j;
         if (n >= g.n_valid) break;
-        float x = v[j];
-        if (g.bias) x += g.bias[n];
-        if (g.epi == kEpiGelu) {
-          if (g.pre_out) g.pre_out[(size_t)m * g.ld_pre_out + n] = x;
-          x = gelu(x);
-        } else if (g.epi == kEpiDGelu) {
-          x *= gelu_grad(g.pre_in[(size_t)m * g.ld_pre_in + n]);
+        if (vec && n + 3 < g.n_valid) {
+          float x[4] = {v[j], v[j + 1], v[j + 2], v[j + 3]};
+          if (g.bias) {  // the bias sits at any offset of the parameter vector
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x[q] += g.bias[n + q];
+          }
+          if (g.epi == kEpiGelu) {
+            if (g.pre_out)
+              *reinterpret_cast<float4 *>(g.pre_out + (size_t)m * g.ld_pre_out + n) =
+                  make_float4(x[0], x[1], x[2], x[3]);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x[q] = gelu(x[q]);
+          } else if (g.epi == kEpiDGelu) {
+            const float4 pi =
+                *reinterpret_cast<const float4 *>(g.pre_in + (size_t)m * g.ld_pre_in + n);
+            x[0] *= gelu_grad(pi.x); x[1] *= gelu_grad(pi.y);
+            x[2] *= gelu_grad(pi.z); x[3] *= gelu_grad(pi.w);
+          }
+          if (out)
+            *reinterpret_cast<float4 *>(out + (size_t)m * g.ldo + n) =
+                make_float4(x[0], x[1], x[2], x[3]);
+          if (g.out_bf || g.out_bt) {
+            __nv_bfloat16 h[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) h[q] = __float2bfloat16_rn(x[q]);
+            if (g.out_bf) {
+              uint2 pk;
+              pk.x = (uint32_t)__bfloat16_as_ushort(h[0]) |
+                     ((uint32_t)__bfloat16_as_ushort(h[1]) << 16);
+              pk.y = (uint32_t)__bfloat16_as_ushort(h[2]) |
+                     ((uint32_t)__bfloat16_as_ushort(h[3]) << 16);
+              *reinterpret_cast<uint2 *>(g.out_bf + (size_t)m * g.ldb_out + n) = pk;
+            }
+            if (g.out_bt)
+#pragma unroll
+              for (int q = 0; q < 4; ++q) g.out_bt[(size_t)(n + q) * g.ldt_out + m] = h[q];
+          }
+          continue;
         }
-        if (out) out[(size_t)m * g.ldo + n] = x;
-        const __nv_bfloat16 h = __float2bfloat16_rn(x);
-        if (g.out_bf) g.out_bf[(size_t)m * g.ldb_out + n] = h;
-        if (g.out_bt) g.out_bt[(size_t)n * g.ldt_out + m] = h;
+        for (int q = 0; q < 4 && n + q < g.n_valid; ++q) {
+          const int nn = n + q;
+          float x = v[j + q];
+          if (g.bias) x += g.bias[nn];
+          if (g.epi == kEpiGelu) {
+            if (g.pre_out) g.pre_out[(size_t)m * g.ld_pre_out + nn] = x;
+            x = gelu(x);
+          } else if (g.epi == kEpiDGelu) {
+            x *= gelu_grad(g.pre_in[(size_t)m * g.ld_pre_in + nn]);
+          }
+          if (out) out[(size_t)m * g.ldo + nn] = x;
+          const __nv_bfloat16 h = __float2bfloat16_rn(x);
+          if (g.out_bf) g.out_bf[(size_t)m * g.ldb_out + nn] = h;
+          if (g.out_bt) g.out_bt[(size_t)nn * g.ldt_out + m] = h;
+        }
       }
     }
   }
@@ -240,7 +325,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_bf16_kernel(GemmArgs g) 
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
 }
 
-inline size_t gemm_smem_bytes(int N) { return (size_t)(kTileM + N) * kKC * 2; }
+// Dynamic shared memory of gemm_bf16_kernel for N columns (two stage buffers).
+inline size_t gemm_smem_bytes(int N) { return 2 * (size_t)(kTileM + N) * kKC * 2; }
 
 }  // namespace tc
 }  // namespace lddmm

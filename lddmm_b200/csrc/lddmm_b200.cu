@@ -663,15 +663,24 @@ static HostPlan plan_sweeps(const std::vector<int2> &units, const std::vector<Pa
   return h;
 }
 
-static int default_cluster(int n_items) {
-  // aim for >= ~8 CTAs per SM of 148 SMs, and split in two while there are fewer than
-  // 32 tiles per SM: more, shorter CTAs even out the SMs' loads at the end of the
-  // sweep (measured with per-step sweeps: 40,962 landmarks 12 % and 163,842 landmarks
-  // 3 % faster per evaluation than one CTA per tile; four-way splits were slower)
+static int default_cluster(int n_items, int sms = 148) {
+  // aim for >= ~8 CTAs per SM, and split in two while there are fewer than 32 tiles
+  // per SM: more, shorter CTAs even out the SMs' loads at the end of the sweep
+  // (measured with per-step sweeps on 148 SMs: 40,962 landmarks 12 % and 163,842
+  // landmarks 3 % faster per evaluation than one CTA per tile; four-way splits were
+  // slower)
   int S = 1;
-  while (S < 8 && n_items * S < 1200) S *= 2;
-  if (S == 1 && n_items < 148 * 32) S = 2;
+  while (S < 8 && n_items * S < 8 * sms) S *= 2;
+  if (S == 1 && n_items < 32 * sms) S = 2;
   return S;
+}
+
+static int device_sms(int dev) {
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      sms <= 0)
+    sms = 148;
+  return sms;
 }
 
 static cudaError_t run_eval(lddmm_ctx &c, double *g_out, double *f_out, double *vlc,
@@ -999,9 +1008,11 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   }
   CU(cudaMemcpyAsync(c.pd, c.hpd.data(), sizeof(PairDesc) * num, cudaMemcpyHostToDevice, c.stream));
 
-  c.S_shoot = cf.cluster_shoot > 0 ? cf.cluster_shoot : default_cluster(c.n_pt_items);
-  c.S_adj = cf.cluster_adjoint > 0 ? cf.cluster_adjoint : default_cluster(c.n_pt_items);
-  c.S_vfd = cf.cluster_varifold > 0 ? cf.cluster_varifold : default_cluster(c.n_el_items);
+  const int dev_sms = device_sms(c.device);
+  c.S_shoot = cf.cluster_shoot > 0 ? cf.cluster_shoot : default_cluster(c.n_pt_items, dev_sms);
+  c.S_adj = cf.cluster_adjoint > 0 ? cf.cluster_adjoint : default_cluster(c.n_pt_items, dev_sms);
+  c.S_vfd =
+      cf.cluster_varifold > 0 ? cf.cluster_varifold : default_cluster(c.n_el_items, dev_sms);
   if (cf.cluster_varifold <= 0 && c.has_vfd && c.vfd_clusters) {
     // the largest split whose clusters all fit in one resident wave (clusters are
     // placed within a GPC, so the count comes from cudaOccupancyMaxActiveClusters; a
@@ -1894,6 +1905,7 @@ struct CrossRun {
   double fac;
   double *out;
   const int2 *items;
+  int sms = 148;  // the current device's SM count (set by the caller)
   template <int D, int ORDER>
   cudaError_t run() {
     const int ntiles = na_pad / kTile;
@@ -1901,12 +1913,12 @@ struct CrossRun {
       CrossOp<D, ORDER, kCrossMul> op;
       op.qa = qa; op.xa = xa; op.qb = qb; op.yb = yb;
       op.na = na; op.nb_pad = nb_pad; op.fac = fac; op.out = out;
-      return launch_sweep(op, items, ntiles, default_cluster(ntiles), st);
+      return launch_sweep(op, items, ntiles, default_cluster(ntiles, sms), st);
     }
     CrossOp<D, ORDER, kCrossDq> op;
     op.qa = qa; op.xa = xa; op.qb = qb; op.yb = yb;
     op.na = na; op.nb_pad = nb_pad; op.fac = fac; op.out = out;
-    return launch_sweep(op, items, ntiles, default_cluster(ntiles), st);
+    return launch_sweep(op, items, ntiles, default_cluster(ntiles, sms), st);
   }
 };
 
@@ -1917,9 +1929,9 @@ struct MatrixRun {
   double *K;
   template <int D, int ORDER>
   cudaError_t run() {
-    int dev = 0, sms = 148;
+    int dev = 0;
     cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int sms = device_sms(dev);
     const long long total = (long long)ni * nj;
     const long long want = (total + 255) / 256;
     const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(want, 8LL * sms));
@@ -1981,6 +1993,9 @@ extern "C" int lddmm_multiply_kernel2(int dim, int ni, const double *qi, int nj,
   CU(w.put_items(&items, ni_pad / kTile));
   CU(w.alloc(&dv, (size_t)ni * dim));
   CrossRun r{w.st, kCrossMul, dqi, nullptr, dqj, da, ni, ni_pad, nj_pad, 1.0, dv, items};
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  r.sms = device_sms(dev);
   CU(with_kernel(dim, order, r));
   CU(cudaMemcpyAsync(v, dv, sizeof(double) * ni * dim, cudaMemcpyDeviceToHost, w.st));
   CU(cudaStreamSynchronize(w.st));
@@ -2014,9 +2029,13 @@ extern "C" int lddmm_dq_kernel2(int dim, int ni, const double *qi, int nj, const
   CU(w.alloc(&oi, (size_t)ni * dim));
   CU(w.alloc(&oj, (size_t)nj * dim));
   // i side: rows qi with l, columns qj with r; j side: rows qj with r, columns qi with l
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
   CrossRun a{w.st, kCrossDq, dqi_s, dl, dqj_s, dr, ni, ni_pad, nj_pad, pd_fac, oi, items_i};
+  a.sms = device_sms(dev);
   CU(with_kernel(dim, order, a));
   CrossRun b{w.st, kCrossDq, dqj_s, dr, dqi_s, dl, nj, nj_pad, ni_pad, pd_fac, oj, items_j};
+  b.sms = a.sms;
   CU(with_kernel(dim, order, b));
   CU(cudaMemcpyAsync(dqi, oi, sizeof(double) * ni * dim, cudaMemcpyDeviceToHost, w.st));
   CU(cudaMemcpyAsync(dqj, oj, sizeof(double) * nj * dim, cudaMemcpyDeviceToHost, w.st));

@@ -160,6 +160,88 @@ __device__ __forceinline__ void stage_async(unsigned char *dst, const __nv_bfloa
   }
 }
 
+// Epilogue of one 128-row tile: the accumulator (TMEM, warp w owns lanes 32w..32w+31
+// = rows m0 + 32w ..) through bias / GELU / GELU' into the outputs of `g`; `out` is the
+// FP32 output of this K split (or null).  Called by all 4 warps after the tile's MMAs
+// completed and tcgen05.fence::after_thread_sync.
+__device__ __forceinline__ void gemm_epilogue(const GemmArgs &g, int m0, uint32_t tmem,
+                                              float *out) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m = m0 + warp * 32 + lane;
+  const bool row_ok = m < g.M;
+  // four columns per store where every output in use allows it
+  const bool vec =
+      (!out || (((uintptr_t)out & 15u) == 0 && (g.ldo & 3) == 0)) &&
+      (!g.pre_out || (((uintptr_t)g.pre_out & 15u) == 0 && (g.ld_pre_out & 3) == 0)) &&
+      (!g.out_bf || (((uintptr_t)g.out_bf & 7u) == 0 && (g.ldb_out & 3) == 0)) &&
+      (g.epi != kEpiDGelu ||
+       (((uintptr_t)g.pre_in & 15u) == 0 && (g.ld_pre_in & 3) == 0));
+  for (int c0 = 0; c0 < g.N; c0 += 32) {
+    float v[32];
+    tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+    if (!row_ok) continue;
+#pragma unroll
+    for (int j = 0; j < 32; j += 4) {
+      const int n = c0 + j;
+      if (n >= g.n_valid) break;
+      if (vec && n + 3 < g.n_valid) {
+        float x[4] = {v[j], v[j + 1], v[j + 2], v[j + 3]};
+        if (g.bias) {  // the bias sits at any offset of the parameter vector
+#pragma unroll
+          for (int q = 0; q < 4; ++q) x[q] += g.bias[n + q];
+        }
+        if (g.epi == kEpiGelu) {
+          if (g.pre_out)
+            *reinterpret_cast<float4 *>(g.pre_out + (size_t)m * g.ld_pre_out + n) =
+                make_float4(x[0], x[1], x[2], x[3]);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) x[q] = gelu(x[q]);
+        } else if (g.epi == kEpiDGelu) {
+          const float4 pi =
+              *reinterpret_cast<const float4 *>(g.pre_in + (size_t)m * g.ld_pre_in + n);
+          x[0] *= gelu_grad(pi.x); x[1] *= gelu_grad(pi.y);
+          x[2] *= gelu_grad(pi.z); x[3] *= gelu_grad(pi.w);
+        }
+        if (out)
+          *reinterpret_cast<float4 *>(out + (size_t)m * g.ldo + n) =
+              make_float4(x[0], x[1], x[2], x[3]);
+        if (g.out_bf || g.out_bt) {
+          __nv_bfloat16 h[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) h[q] = __float2bfloat16_rn(x[q]);
+          if (g.out_bf) {
+            uint2 pk;
+            pk.x = (uint32_t)__bfloat16_as_ushort(h[0]) |
+                   ((uint32_t)__bfloat16_as_ushort(h[1]) << 16);
+            pk.y = (uint32_t)__bfloat16_as_ushort(h[2]) |
+                   ((uint32_t)__bfloat16_as_ushort(h[3]) << 16);
+            *reinterpret_cast<uint2 *>(g.out_bf + (size_t)m * g.ldb_out + n) = pk;
+          }
+          if (g.out_bt)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) g.out_bt[(size_t)(n + q) * g.ldt_out + m] = h[q];
+        }
+        continue;
+      }
+      for (int q = 0; q < 4 && n + q < g.n_valid; ++q) {
+        const int nn = n + q;
+        float x = v[j + q];
+        if (g.bias) x += g.bias[nn];
+        if (g.epi == kEpiGelu) {
+          if (g.pre_out) g.pre_out[(size_t)m * g.ld_pre_out + nn] = x;
+          x = gelu(x);
+        } else if (g.epi == kEpiDGelu) {
+          x *= gelu_grad(g.pre_in[(size_t)m * g.ld_pre_in + nn]);
+        }
+        if (out) out[(size_t)m * g.ldo + nn] = x;
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        if (g.out_bf) g.out_bf[(size_t)m * g.ldb_out + nn] = h;
+        if (g.out_bt) g.out_bt[(size_t)nn * g.ldt_out + m] = h;
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kGemmThreads, 1) gemm_bf16_kernel(GemmArgs g) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const size_t stage_bytes = (size_t)(kTileM + g.N) * kKC * 2;
@@ -243,86 +325,129 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_bf16_kernel(GemmArgs g) 
   for (int j = done + 1; j < issued; ++j) wait_mma(j);
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (s_ok && issued > 0) {
-    const int m = m0 + warp * 32 + lane;
-    const bool row_ok = m < g.M;
-    float *out = g.out ? g.out + (size_t)blockIdx.y * g.split_stride : nullptr;
-    // four columns per store where every output in use allows it
-    const bool vec =
-        (!out || (((uintptr_t)out & 15u) == 0 && (g.ldo & 3) == 0)) &&
-        (!g.pre_out || (((uintptr_t)g.pre_out & 15u) == 0 && (g.ld_pre_out & 3) == 0)) &&
-        (!g.out_bf || (((uintptr_t)g.out_bf & 7u) == 0 && (g.ldb_out & 3) == 0)) &&
-        (g.epi != kEpiDGelu ||
-         (((uintptr_t)g.pre_in & 15u) == 0 && (g.ld_pre_in & 3) == 0));
-    for (int c0 = 0; c0 < g.N; c0 += 32) {
-      float v[32];
-      tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-      if (!row_ok) continue;
-#pragma unroll
-      for (int j = 0; j < 32; j += 4) {
-        const int n = c0 + j;
-        if (n >= g.n_valid) break;
-        if (vec && n + 3 < g.n_valid) {
-          float x[4] = {v[j], v[j + 1], v[j + 2], v[j + 3]};
-          if (g.bias) {  // the bias sits at any offset of the parameter vector
-#pragma unroll
-            for (int q = 0; q < 4; ++q) x[q] += g.bias[n + q];
-          }
-          if (g.epi == kEpiGelu) {
-            if (g.pre_out)
-              *reinterpret_cast<float4 *>(g.pre_out + (size_t)m * g.ld_pre_out + n) =
-                  make_float4(x[0], x[1], x[2], x[3]);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) x[q] = gelu(x[q]);
-          } else if (g.epi == kEpiDGelu) {
-            const float4 pi =
-                *reinterpret_cast<const float4 *>(g.pre_in + (size_t)m * g.ld_pre_in + n);
-            x[0] *= gelu_grad(pi.x); x[1] *= gelu_grad(pi.y);
-            x[2] *= gelu_grad(pi.z); x[3] *= gelu_grad(pi.w);
-          }
-          if (out)
-            *reinterpret_cast<float4 *>(out + (size_t)m * g.ldo + n) =
-                make_float4(x[0], x[1], x[2], x[3]);
-          if (g.out_bf || g.out_bt) {
-            __nv_bfloat16 h[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) h[q] = __float2bfloat16_rn(x[q]);
-            if (g.out_bf) {
-              uint2 pk;
-              pk.x = (uint32_t)__bfloat16_as_ushort(h[0]) |
-                     ((uint32_t)__bfloat16_as_ushort(h[1]) << 16);
-              pk.y = (uint32_t)__bfloat16_as_ushort(h[2]) |
-                     ((uint32_t)__bfloat16_as_ushort(h[3]) << 16);
-              *reinterpret_cast<uint2 *>(g.out_bf + (size_t)m * g.ldb_out + n) = pk;
-            }
-            if (g.out_bt)
-#pragma unroll
-              for (int q = 0; q < 4; ++q) g.out_bt[(size_t)(n + q) * g.ldt_out + m] = h[q];
-          }
-          continue;
-        }
-        for (int q = 0; q < 4 && n + q < g.n_valid; ++q) {
-          const int nn = n + q;
-          float x = v[j + q];
-          if (g.bias) x += g.bias[nn];
-          if (g.epi == kEpiGelu) {
-            if (g.pre_out) g.pre_out[(size_t)m * g.ld_pre_out + nn] = x;
-            x = gelu(x);
-          } else if (g.epi == kEpiDGelu) {
-            x *= gelu_grad(g.pre_in[(size_t)m * g.ld_pre_in + nn]);
-          }
-          if (out) out[(size_t)m * g.ldo + nn] = x;
-          const __nv_bfloat16 h = __float2bfloat16_rn(x);
-          if (g.out_bf) g.out_bf[(size_t)m * g.ldb_out + nn] = h;
-          if (g.out_bt) g.out_bt[(size_t)nn * g.ldt_out + m] = h;
-        }
-      }
-    }
-  }
+  if (s_ok && issued > 0)
+    gemm_epilogue(g, m0, tmem, g.out ? g.out + (size_t)blockIdx.y * g.split_stride : nullptr);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
+
+// Weight-resident form for the common case of one K split with K <= kResK and
+// N <= 256 (every layer of the warm-start network): persistent CTAs, one per SM, loop
+// over 128-row tiles (tile = blockIdx.x + i * gridDim.x).  B (the weights, at most
+// 128 KB) is staged into shared memory once; A streams through kResStages cp.async
+// buffers in a global sequence of (tile, K-chunk) steps, a buffer refilled only after
+// the mbarrier of the MMAs that read it completed; the loads of the next tile's first
+// chunks are in flight while a tile's epilogue runs.  Every MMA commit is waited
+// exactly once, in order (wait_upto), with bounded waits.
+constexpr int kResK = 256;
+constexpr int kResStages = 3;
+
+__global__ void __launch_bounds__(kGemmThreads, 1) gemm_bf16_resident_kernel(GemmArgs g) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int nk = (g.K + kKC - 1) / kKC;                     // K chunks per tile
+  const size_t b_chunk = (size_t)g.N * kKC * 2;             // bytes of one B chunk
+  unsigned char *sBres = smem;                               // nk B chunks
+  unsigned char *sAst = smem + (size_t)nk * b_chunk;         // kResStages A chunks
+  __shared__ uint64_t s_mbar[kResStages];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_ok;
+  const int warp = threadIdx.x >> 5;
+  const int ntiles = (g.M + kTileM - 1) / kTileM;
+  const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int Q = my_tiles * nk;                               // (tile, chunk) steps
+  const uint32_t ncols = g.N <= 32 ? 32u : g.N <= 64 ? 64u : g.N <= 128 ? 128u : 256u;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < kResStages; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[b])));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_ok = 1;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+  const uint32_t idesc = instr_desc_bf16(kTileM, g.N);
+  // B, all K chunks, one cp.async group (it completes before every later group)
+  for (int kc = 0; kc < nk; ++kc)
+    stage_async(sBres + kc * b_chunk, g.B, g.ldb, 0, g.N, g.N, kc * kKC, g.K);
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  auto issue_a = [&](int q) {  // step q: tile blockIdx.x + (q / nk) gridDim.x, chunk q % nk
+    const int tile = blockIdx.x + (q / nk) * gridDim.x;
+    stage_async(sAst + (size_t)(q % kResStages) * kTileM * kKC * 2, g.A, g.lda, tile * kTileM,
+                kTileM, g.M, (q % nk) * kKC, g.K);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  int waited = 0;  // MMA steps 0 .. waited - 1 are complete
+  auto wait_upto = [&](int j) {
+    for (; waited <= j; ++waited)
+      if (!mbar_wait(&s_mbar[waited % kResStages], (uint32_t)((waited / kResStages) & 1))) {
+        s_ok = 0;
+        if (g.error) atomicExch(g.error, 1u);
+      }
+  };
+  for (int q = 0; q < kResStages - 1 && q < Q; ++q) issue_a(q);
+  int issued = 0;
+  for (int q = 0; q < Q; ++q) {
+    // A chunk q has landed once at most the groups of the chunks after it are pending
+    const int pending = min(Q - 1, q + kResStages - 2) - q;
+    if (pending >= 1)
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    else
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    const int kc = q % nk;
+    if (threadIdx.x == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = smem_u32(sAst + (size_t)(q % kResStages) * kTileM * kKC * 2);
+      const uint32_t b0 = smem_u32(sBres + kc * b_chunk);
+#pragma unroll
+      for (int s = 0; s < kKC / 16; ++s) {
+        const uint64_t da = smem_desc(a0 + s * 256, 128, kKC * 16);
+        const uint64_t db = smem_desc(b0 + s * 256, 128, kKC * 16);
+        mma_bf16(tmem, da, db, idesc, (kc == 0 && s == 0) ? 0u : 1u);
+      }
+      mma_commit(&s_mbar[q % kResStages]);
+    }
+    ++issued;
+    // refill the buffer of step q - 1 with step q + kResStages - 1 once its MMAs are done
+    if (q + kResStages - 1 < Q) {
+      if (q >= 1) wait_upto(q - 1);
+      __syncthreads();
+      if (!s_ok) break;
+      issue_a(q + kResStages - 1);
+    }
+    if (kc == nk - 1) {
+      // the tile's accumulation is complete once its last commit is
+      wait_upto(q);
+      __syncthreads();
+      if (!s_ok) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      gemm_epilogue(g, (blockIdx.x + (q / nk) * gridDim.x) * kTileM, tmem, g.out);
+      // the next tile's first MMA overwrites the accumulator
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+    }
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  wait_upto(issued - 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
+
+inline size_t gemm_resident_smem_bytes(int N, int K) {
+  const int nk = (K + kKC - 1) / kKC;
+  return (size_t)nk * N * kKC * 2 + (size_t)kResStages * kTileM * kKC * 2;
 }
 
 // Dynamic shared memory of gemm_bf16_kernel for N columns (two stage buffers).

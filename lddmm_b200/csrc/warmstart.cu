@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -341,13 +342,42 @@ cudaError_t refresh_bf16(lddmm_ws &w) {
   return cudaGetLastError();
 }
 
+// Launches C = A . B^T on `st`: the weight-resident persistent kernel when there is one
+// K split with K <= kResK (every layer's forward and input-gradient products), else
+// the per-tile kernel (split-K weight gradients).  Both kernels' shared-memory limits
+// are raised once per device.
+cudaError_t launch_gemm(GemmArgs a, int splits, cudaStream_t st) {
+  static std::atomic<bool> attr_set[64];  // zero-initialised; setting twice is harmless
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 0 && dev < 64 && !attr_set[dev].load()) {
+    e = cudaFuncSetAttribute(gemm_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)gemm_smem_bytes(256));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(gemm_bf16_resident_kernel,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)gemm_resident_smem_bytes(256, kResK));
+    if (e != cudaSuccess) return e;
+    attr_set[dev].store(true);
+  }
+  if (a.k_split <= 0) a.k_split = (a.K + kKC - 1) / kKC * kKC;
+  const int ntiles = (a.M + kTileM - 1) / kTileM;
+  if (splits == 1 && a.K <= kResK && a.k_split >= a.K && a.N <= 256 && ntiles > 0) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = std::min(ntiles, std::max(sms, 1));
+    gemm_bf16_resident_kernel<<<grid, kGemmThreads, gemm_resident_smem_bytes(a.N, a.K), st>>>(a);
+  } else {
+    gemm_bf16_kernel<<<dim3(ntiles, splits), kGemmThreads, gemm_smem_bytes(a.N), st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
 // C = A . B^T through the tensor-core GEMM (see tc_gemm.cuh)
 cudaError_t gemm(lddmm_ws &w, GemmArgs a, int splits) {
   a.error = w.err;
-  if (a.k_split <= 0) a.k_split = (a.K + kKC - 1) / kKC * kKC;
-  dim3 grid((a.M + kTileM - 1) / kTileM, splits);
-  gemm_bf16_kernel<<<grid, kGemmThreads, gemm_smem_bytes(a.N), w.stream>>>(a);
-  return cudaGetLastError();
+  return launch_gemm(a, splits, w.stream);
 }
 
 GemmArgs fwd_args(const bf16 *A, long long lda, const Layer &l, long long M) {
@@ -747,8 +777,6 @@ extern "C" int lddmm_ws_gemm_bf16(const void *d_a, long long lda, const void *d_
            "leading dimensions multiples of 8");
     return LDDMM_ERR_ARG;
   }
-  WCU(cudaFuncSetAttribute(gemm_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)gemm_smem_bytes(256)));
   GemmArgs a = {};
   a.A = (const bf16 *)d_a;
   a.lda = lda;
@@ -761,8 +789,6 @@ extern "C" int lddmm_ws_gemm_bf16(const void *d_a, long long lda, const void *d_
   a.k_split = (k + kKC - 1) / kKC * kKC;
   a.out = d_c;
   a.ldo = ldc;
-  cudaStream_t st = (cudaStream_t)stream;
-  gemm_bf16_kernel<<<dim3((m + kTileM - 1) / kTileM, 1), kGemmThreads, gemm_smem_bytes(n), st>>>(a);
-  WCU(cudaGetLastError());
+  WCU(launch_gemm(a, 1, (cudaStream_t)stream));
   return 0;
 }

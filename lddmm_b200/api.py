@@ -116,12 +116,20 @@ class Context:
 
     def lbfgs(self, alp0, itr_max=1000, tol=1e-6, wolfe1=1e-4, wolfe2=0.9, mem_num=5,
               verbose=False, rel_obj_tol=0.0):
+        """L-BFGS from alp0 for every pair of the batch (Cpp/src/LBFGS.cpp:25).
+        Returns the final momenta and one dict per pair (f, glen, status, iters,
+        evals).  A pair's own outcome is its ``status``: 0, the line-search codes 1-3,
+        or -3 (LDDMM_ERR_NONFINITE) for a pair whose objective was not finite; those
+        do not raise, so the other pairs' results stay available.  Errors of the call
+        itself (arguments, CUDA, timeouts, memory) raise LddmmError."""
         x = np.ascontiguousarray(alp0, dtype=np.float64).reshape(-1).copy()
         if x.size != self.var_total:
             raise ValueError(f"alp0 has {x.size} values, the batch {self.var_total}")
         opt = _lib.Opt(itr_max, tol, wolfe1, wolfe2, mem_num, 1 if verbose else 0, rel_obj_tol)
         res = (_lib.Result * self.P)()
-        check(lib.lddmm_lbfgs(self._h, C.byref(opt), dptr(x), res))
+        rc = lib.lddmm_lbfgs(self._h, C.byref(opt), dptr(x), res)
+        if rc < 0 and rc != -3:
+            check(rc)
         out = [dict(f=r.fcn, glen=r.grd_len, status=r.status, iters=r.iters, evals=r.evals)
                for r in res]
         return x, out

@@ -118,6 +118,12 @@ def test_lbfgs_nonfinite_pair_fails_alone(api):
         x1, r1 = c1.lbfgs(np.zeros(probs[1].var_num), itr_max=25)
     assert res[1].iters == r1[0]["iters"] and res[1].fcn == r1[0]["f"]
     assert np.array_equal(xs[1], x1)
+    # the Python API reports the failed pair in its status instead of raising
+    with api.Context(probs, **shape) as ctx:
+        x = np.zeros(ctx.var_total)
+        x[0] = np.nan
+        xp, rp = ctx.lbfgs(x, itr_max=25)
+    assert [r["status"] for r in rp] == [-3, 0] and rp[1]["f"] == r1[0]["f"]
 
 
 def test_lbfgs_graph_and_direct_launches_agree(api):

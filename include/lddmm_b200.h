@@ -160,6 +160,11 @@ int lddmm_lbfgs_device(lddmm_ctx *ctx, const lddmm_opt *opt, double *d_alp_inout
  * (f, |g|, step length, evaluations in the line search), row 0 the initial point.
  * Returns the number of rows written (at most cap). */
 int lddmm_lbfgs_trace(const lddmm_ctx *ctx, int pair, double *rows4, int cap);
+/* Gradient at each pair's last accepted point of the last lddmm_lbfgs /
+ * lddmm_lbfgs_device call (the reference's grdNow, Cpp/src/LBFGS.cpp:25), in the
+ * variable layout, concatenated like alp; host memory of lddmm_ctx_var_total doubles.
+ * LDDMM_ERR_ARG before the first L-BFGS call of the context. */
+int lddmm_lbfgs_grad(const lddmm_ctx *ctx, double *grd);
 
 /* Trajectory of every pair: nde_stk (dim x N x time_num per pair) and velocities
  * vlc_stk (dim x N x (time_num - 1) per pair), concatenated by pair.  Either output

@@ -27,7 +27,7 @@ EXPORTS = [
     "lddmm_ws_create", "lddmm_ws_destroy", "lddmm_ws_last_error", "lddmm_ws_num_params",
     "lddmm_ws_params", "lddmm_ws_grad", "lddmm_ws_train_step", "lddmm_ws_predict",
     "lddmm_ws_gemm_bf16", "lddmm_wait_selftest", "lddmm_compute_kernel",
-    "lddmm_multiply_kernel2", "lddmm_dq_kernel2",
+    "lddmm_multiply_kernel2", "lddmm_dq_kernel2", "lddmm_lbfgs_grad",
 ]
 
 ERRORS = {
@@ -93,6 +93,7 @@ def _load():
     L.lddmm_lbfgs.argtypes = [C.c_void_p, C.POINTER(Opt), _dp, C.POINTER(Result)]
     L.lddmm_lbfgs_device.argtypes = [C.c_void_p, C.POINTER(Opt), C.c_void_p, C.POINTER(Result)]
     L.lddmm_lbfgs_trace.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
+    L.lddmm_lbfgs_grad.argtypes = [C.c_void_p, _dp]
     L.lddmm_shoot.argtypes = [C.c_void_p, _dp, _dp, _dp]
     L.lddmm_LDDMM.argtypes = [C.c_int] * 5 + [_dp, _dp, _ip, _ip, _dp, _dp, _dp, C.c_char,
                                                C.c_double, C.c_char, C.c_double, C.c_double,

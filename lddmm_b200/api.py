@@ -134,6 +134,13 @@ class Context:
                for r in res]
         return x, out
 
+    def lbfgs_grad(self):
+        """Gradient at the last accepted point of the last ``lbfgs`` call (the
+        reference's grdNow), concatenated over the pairs like the momenta."""
+        g = np.zeros(self.var_total)
+        check(lib.lddmm_lbfgs_grad(self._h, dptr(g)))
+        return g
+
     def trace(self, pair=0, cap=100001):
         rows = np.zeros((cap, 4))
         n = check(lib.lddmm_lbfgs_trace(self._h, pair, dptr(rows), cap))

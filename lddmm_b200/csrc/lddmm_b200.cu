@@ -1572,6 +1572,20 @@ extern "C" int lddmm_lbfgs_trace(const lddmm_ctx *ctx, int pair, double *rows4, 
   return n;
 }
 
+extern "C" int lddmm_lbfgs_grad(const lddmm_ctx *ctx, double *grd) {
+  if (!ctx || !grd || !ctx->G) {
+    set_err("lddmm_lbfgs_grad: bad arguments or no L-BFGS call yet");
+    return LDDMM_ERR_ARG;
+  }
+  if (cudaMemcpyAsync(grd, ctx->G, sizeof(double) * ctx->nvar, cudaMemcpyDeviceToHost,
+                      ctx->stream) != cudaSuccess ||
+      cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+    set_err("lddmm_lbfgs_grad: %s", cudaGetErrorString(cudaGetLastError()));
+    return LDDMM_ERR_CUDA;
+  }
+  return 0;
+}
+
 extern "C" int lddmm_ctx_timeline(const lddmm_ctx *ctx, double *us6) {
   if (!ctx || !us6 || !ctx->sync) return LDDMM_ERR_ARG;
   StepSync h;

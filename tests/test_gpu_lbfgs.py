@@ -126,6 +126,20 @@ def test_lbfgs_nonfinite_pair_fails_alone(api):
     assert [r["status"] for r in rp] == [-3, 0] and rp[1]["f"] == r1[0]["f"]
 
 
+def test_lbfgs_grad_is_the_gradient_at_the_returned_point(api):
+    """lddmm_lbfgs_grad returns the reference's grdNow: the gradient at the last
+    accepted point, the same evaluation objgrd gives there."""
+    from lddmm_b200 import problem
+
+    P = problem.circle_to_square(n_src=64, n_tgt=64, time_num=6)
+    with api.Context(P) as ctx:
+        x, res = ctx.lbfgs(np.zeros(P.var_num), itr_max=15)
+        g = ctx.lbfgs_grad()
+        f2, g2 = ctx.objgrd(x)
+    assert np.isclose(np.linalg.norm(g), res[0]["glen"], rtol=1e-12)
+    assert f2[0] == res[0]["f"] and np.array_equal(g, g2)
+
+
 def test_lbfgs_graph_and_direct_launches_agree(api):
     from lddmm_b200 import problem
 

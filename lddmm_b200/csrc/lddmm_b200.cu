@@ -156,6 +156,7 @@ struct lddmm_ctx {
   PairState *st = nullptr;
   float4 *qs = nullptr, *as = nullptr, *us = nullptr, *ls = nullptr;
   double *q64 = nullptr, *p64 = nullptr;
+  float4 *dbb = nullptr, *tbb = nullptr;  // 32-element block boxes (varifold culling)
   float4 *ec = nullptr, *en = nullptr, *el = nullptr, *tc = nullptr, *tn = nullptr,
          *tl = nullptr;
   double *e64 = nullptr, *dcdd = nullptr, *tgt64 = nullptr;
@@ -224,6 +225,7 @@ lddmm_ctx::~lddmm_ctx() {
   dfree(rec, stream); dfree(sync, stream); dfree(units, stream); dfree(segs, stream);
   dfree(cta_seg, stream); dfree(unit_parts, stream); dfree(seg_part, stream);
   dfree(unit_cnt, stream);
+  dfree(dbb, stream); dfree(tbb, stream);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
 
@@ -388,6 +390,8 @@ static cudaError_t varifold_impl(lddmm_ctx &c) {
   op.dcdd = c.dcdd;
   op.tile_part = c.vfd_part;
   op.ow2 = c.ow2;
+  op.dbb = c.dbb;
+  op.tbb = c.tbb;
   return launch(sweep_packed_kernel<VarifoldOp<D, CT, DT>, kWarps>,
                 (unsigned)(c.n_el_items * c.S_vfd), kWarps * 32, c.S_vfd, c.stream, op,
                 (const int2 *)c.el_items, c.S_vfd);
@@ -473,9 +477,9 @@ static cudaError_t launch_geometry(lddmm_ctx &c, const double *q64T) {
   const unsigned nb = (unsigned)((c.EDtot + 127) / 128);
   if (c.D == 3)
     return launch(geometry_kernel<3>, nb, 128, 0, c.stream, c.pd, c.act, c.elm, c.EDtot, q64T,
-                  c.ec, c.en, c.el, c.e64);
+                  c.ec, c.en, c.el, c.e64, c.dbb);
   return launch(geometry_kernel<2>, nb, 128, 0, c.stream, c.pd, c.act, c.elm, c.EDtot, q64T, c.ec,
-                c.en, c.el, c.e64);
+                c.en, c.el, c.e64, c.dbb);
 }
 
 static cudaError_t launch_gather(lddmm_ctx &c, const double *q64T, float4 *un, float4 *ln,
@@ -809,6 +813,7 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   std::vector<int> h_ptpair(c.NPtot, -1);
   std::vector<int4> h_elm(std::max(c.EDtot, 1), make_int4(0, 0, 0, -1));
   std::vector<float4> h_tc(std::max(c.ETtot, 1), make_float4(0, 0, 0, 0)), h_tn(h_tc), h_tl(h_tc);
+  std::vector<char> h_treal(std::max(c.ETtot, 1), 0);  // real (not padding) target element
   std::vector<double> h_tgt64((size_t)std::max(c.ETtot, 1) * 8, 0.0);
   std::vector<int> h_adjptr(c.NPtot + 1, 0);
   std::vector<int4> h_adj;
@@ -846,6 +851,7 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
         lo[d] = (float)(x - (double)hi[d]);
       }
       h_tc[g] = make_float4(hi[0], hi[1], hi[2], (float)(-vol));
+      h_treal[g] = 1;
       h_tl[g] = make_float4(lo[0], lo[1], lo[2], 0.0f);
       h_tn[g] = make_float4((float)nn[0], (float)nn[1], (float)nn[2], 0.0f);
       double *t8 = &h_tgt64[(size_t)g * 8];
@@ -920,6 +926,8 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   CU(dalloc(c.stream, &c.tc, std::max(c.ETtot, 1)));
   CU(dalloc(c.stream, &c.tn, std::max(c.ETtot, 1)));
   CU(dalloc(c.stream, &c.tl, std::max(c.ETtot, 1)));
+  CU(dalloc(c.stream, &c.dbb, (size_t)std::max(c.EDtot / 32, 1) * 2));
+  CU(dalloc(c.stream, &c.tbb, (size_t)std::max(c.ETtot / 32, 1) * 2));
   CU(dalloc(c.stream, &c.e64, (size_t)std::max(c.EDtot, 1) * 4));
   CU(dalloc(c.stream, &c.dcdd, (size_t)std::max(c.EDtot, 1) * 2 * D));
   CU(dalloc(c.stream, &c.tgt64, h_tgt64.size()));
@@ -951,6 +959,29 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
                      cudaMemcpyHostToDevice, c.stream));
   CU(cudaMemcpyAsync(c.tl, h_tl.data(), sizeof(float4) * h_tl.size(),
                      cudaMemcpyHostToDevice, c.stream));
+  {
+    // bounding boxes of the target blocks' scaled centres (hi + lo), real elements only
+    // (a block of padding gets an empty box; a non-finite centre, the whole space);
+    // constant for the context (the deformed blocks' boxes come with the geometry)
+    std::vector<float4> h_tbb((size_t)std::max(c.ETtot / 32, 1) * 2);
+    for (int b = 0; b < c.ETtot / 32; ++b) {
+      float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+      for (int k = 32 * b; k < 32 * b + 32; ++k) {
+        if (!h_treal[k]) continue;
+        const float x[3] = {h_tc[k].x + h_tl[k].x, h_tc[k].y + h_tl[k].y, h_tc[k].z + h_tl[k].z};
+        for (int d = 0; d < 3; ++d) {
+          const bool fin = std::isfinite(x[d]);
+          lo[d] = std::min(lo[d], fin ? x[d] : -INFINITY);
+          hi[d] = std::max(hi[d], fin ? x[d] : INFINITY);
+        }
+      }
+      h_tbb[2 * b] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+      h_tbb[2 * b + 1] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+    }
+    CU(cudaMemcpyAsync(c.tbb, h_tbb.data(), sizeof(float4) * h_tbb.size(),
+                       cudaMemcpyHostToDevice, c.stream));
+    CU(cudaStreamSynchronize(c.stream));  // h_tbb goes out of scope
+  }
   CU(cudaMemcpyAsync(c.tgt64, h_tgt64.data(), sizeof(double) * h_tgt64.size(),
                      cudaMemcpyHostToDevice, c.stream));
   CU(cudaMemcpyAsync(c.adj_ptr, h_adjptr.data(), sizeof(int) * h_adjptr.size(),

@@ -83,6 +83,7 @@ struct ShootOp {
     acc[1] = fmaf(K, w[1].y, acc[1]);
     if (D == 3) acc[D - 1] = fmaf(K, w[1].z, acc[D - 1]);
   }
+  static constexpr bool kCull = false;
   // ---- packed form (sweep_packed_kernel): a lane's two rows in one FP32x2 operation,
   // bitwise the scalar pair() per row (x - y == x + (-y); the scalar nr2, built with
   // fma(-d, d, .), is exactly -(the sum of fma(d, d, .))).  Staged j point, each value
@@ -290,6 +291,7 @@ struct AdjointOp {
       acc[D + d] = fmaf(s, dq[d], acc[D + d]);
     }
   }
+  static constexpr bool kCull = false;
   // ---- packed form (sweep_packed_kernel): a lane's two rows in one FP32x2 operation,
   // bitwise the scalar pair() per row (same operations in the same order; x - y is
   // computed as x + (-y), and nr2 as -(the sum of fma(d, d, .))).  Staged j point,
@@ -453,6 +455,41 @@ struct VarifoldOp {
   double *dcdd;           // out: dc (D), dd (D) per deformed element [EDtot * 2D]
   double *tile_part;      // varifold value per element tile
   float ow2;              // 2 / dirKnlWidth^2 (Gaussian direction kernels)
+  // Distance culling (Gaussian centre kernel only): bounding boxes (lo, hi) of the
+  // scaled centres of every 32-element block, deformed (dbb, per EDtot / 32) and
+  // target (tbb, per ETtot / 32).  A staged 32-column sub-tile whose boxes are farther
+  // than kCullR2 (scaled squared distance) from the row tile's box is skipped: its
+  // centre factors are below 2^-kCullR2 and its direction factors at most 1, so every
+  // skipped term is below 2^-64 of its pair weight, far below FP32 resolution of a row
+  // sum that holds the row's own term (k = 1).
+  const float4 *dbb, *tbb;
+  static constexpr bool kCull = (CT == 'G');
+  static constexpr float kCullR2 = 64.0f;
+  __device__ void row_box(int p, int tile, float (&bx)[6]) const {
+    const int b = pd[p].el_off / 32 + 2 * tile;
+    const float4 l0 = dbb[2 * b], h0 = dbb[2 * b + 1], l1 = dbb[2 * b + 2], h1 = dbb[2 * b + 3];
+    bx[0] = fminf(l0.x, l1.x); bx[1] = fminf(l0.y, l1.y); bx[2] = fminf(l0.z, l1.z);
+    bx[3] = fmaxf(h0.x, h1.x); bx[4] = fmaxf(h0.y, h1.y); bx[5] = fmaxf(h0.z, h1.z);
+  }
+  __device__ __forceinline__ const float4 *col_box(int p, int j) const {
+    const PairDesc &P = pd[p];
+    return j < P.Edpad ? dbb + 2 * ((P.el_off + j) / 32)
+                       : tbb + 2 * ((P.tg_off + j - P.Edpad) / 32);
+  }
+  // true when every column of [j0, j0 + cnt) is beyond the cut-off from the row box
+  __device__ __forceinline__ bool far(int p, const float *rb, int j0, int cnt) const {
+    const float4 *a = col_box(p, j0), *b = col_box(p, j0 + cnt - 1);
+    const float4 la = a[0], ha = a[1], lb = b[0], hb = b[1];
+    const float lo[3] = {fminf(la.x, lb.x), fminf(la.y, lb.y), fminf(la.z, lb.z)};
+    const float hi[3] = {fmaxf(ha.x, hb.x), fmaxf(ha.y, hb.y), fmaxf(ha.z, hb.z)};
+    float d2 = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const float gap = fmaxf(0.0f, fmaxf(lo[d] - rb[3 + d], rb[d] - hi[d]));
+      d2 = fmaf(gap, gap, d2);
+    }
+    return d2 > kCullR2;  // empty boxes give inf gaps
+  }
 
   __device__ bool active(int p) const { return act[p] != 0; }
   __device__ int j_count(int p) const { return pd[p].Edpad + pd[p].Etpad; }
@@ -667,20 +704,15 @@ struct VarifoldOp {
 
 // --------------------------------------------------------- per-element kernels
 
-// landmarksToVarifoldKernel (Cpp/src/varifold3D.cpp:8-39, varifold2D.cpp:8-32), in
-// FP64 from the final positions; writes the FP32 sweep operands and FP64 copies.
+// landmarksToVarifoldKernel (Cpp/src/varifold3D.cpp:8-39, varifold2D.cpp:8-32) for
+// one element, in FP64 from the final positions: centre (double-single, scaled), unit
+// normal / tangent and area / length; writes the FP32 sweep operands and FP64 copies.
+// cf: the scaled centre in FP32, for the block's bounding box.
 template <int D>
-__global__ void geometry_kernel(const PairDesc *__restrict__ pd, const int *__restrict__ act,
-                                const int4 *__restrict__ elm, int n_elm,
-                                const double *__restrict__ q64, float4 *ec, float4 *en,
-                                float4 *el, double *e64) {
-  pdl_wait();
-  pdl_trigger();
-  const int g = blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= n_elm) return;
-  const int4 ev = elm[g];
-  if (ev.w < 0 || !act[ev.w]) return;
-  const PairDesc &P = pd[ev.w];
+__device__ __forceinline__ void geometry_element(const PairDesc &P, int4 ev, int g,
+                                                 const double *__restrict__ q64, float4 *ec,
+                                                 float4 *en, float4 *el, double *e64,
+                                                 float (&cf)[3]) {
   double c[3] = {0, 0, 0}, n[3] = {0, 0, 0}, a;
   if (D == 3) {
     const double *q0 = q64 + (size_t)ev.x * 3, *q1 = q64 + (size_t)ev.y * 3,
@@ -723,6 +755,44 @@ __global__ void geometry_kernel(const PairDesc *__restrict__ pd, const int *__re
   e[1] = n[1];
   e[2] = n[2];
   e[3] = a;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) cf[d] = hi[d] + lo[d];
+}
+
+template <int D>
+__global__ void geometry_kernel(const PairDesc *__restrict__ pd, const int *__restrict__ act,
+                                const int4 *__restrict__ elm, int n_elm,
+                                const double *__restrict__ q64, float4 *ec, float4 *en,
+                                float4 *el, double *e64, float4 *bbox) {
+  pdl_wait();
+  pdl_trigger();
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  const int4 ev = g < n_elm ? elm[g] : make_int4(0, 0, 0, -1);
+  const bool live = ev.w >= 0 && act[ev.w];
+  float cf[3] = {0.0f, 0.0f, 0.0f};
+  if (live) geometry_element<D>(pd[ev.w], ev, g, q64, ec, en, el, e64, cf);
+  // bounding box of the scaled centres of the warp's 32 elements (one block of one
+  // pair: pairs are padded to multiples of 64), for the varifold sweep's distance test.
+  // A block of padding gets an empty box; a non-finite centre widens the box to the
+  // whole space, so that no sub-tile holding it is ever skipped.
+  if (bbox && (g - threadIdx.x % 32) < n_elm) {
+    float lo[3], hi[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const bool fin = isfinite(cf[d]);
+      lo[d] = live ? (fin ? cf[d] : -INFINITY) : INFINITY;
+      hi[d] = live ? (fin ? cf[d] : INFINITY) : -INFINITY;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], off));
+        hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], off));
+      }
+    }
+    if (threadIdx.x % 32 == 0) {
+      bbox[2 * (g / 32)] = make_float4(lo[0], lo[1], lo[2], 0.0f);
+      bbox[2 * (g / 32) + 1] = make_float4(hi[0], hi[1], hi[2], 0.0f);
+    }
+  }
 }
 
 // dqVfdGatherKernel (Cpp/src/varifold3D.cpp:359-391, varifold2D.cpp:337-359) fused

@@ -141,6 +141,11 @@ __global__ void __launch_bounds__(W * 32)
   const int p = it.x, tile = it.y;
   if (!op.active(p)) return;  // identical for every CTA of the cluster
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ float s_rbox[6];  // the row tile's bounding box (ops with distance culling)
+  if constexpr (Op::kCull) {
+    if (threadIdx.x == 0) op.row_box(p, tile, s_rbox);
+    __syncthreads();
+  }
   typename Op::IData2 I;
   op.load_i2(p, tile * kTile + lane, tile * kTile + 32 + lane, I);
   float hi0[NA], lo0[NA], hi1[NA], lo1[NA];
@@ -163,7 +168,11 @@ __global__ void __launch_bounds__(W * 32)
     float2 a[NA];
 #pragma unroll
     for (int k = 0; k < NA; ++k) a[k] = make_float2(0.0f, 0.0f);
-    if (Op::kTwoSets) {
+    bool skip = false;  // warp-uniform: the same rows and sub-tile for every lane
+    if constexpr (Op::kCull) skip = op.far(p, s_rbox, j0, cnt);
+    if (skip) {
+      // every term of the sub-tile is below the cut-off: nothing to add
+    } else if (Op::kTwoSets) {
       const int b = min(max(split - j0, 0), cnt);  // [0, b) first set, [b, cnt) second
       if (b > 0) run_sub2<0>(op, s_j[warp], 0, b, I, a);
       if (b < cnt) run_sub2<1>(op, s_j[warp], b, cnt, I, a);

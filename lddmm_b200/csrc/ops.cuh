@@ -457,8 +457,8 @@ struct VarifoldOp {
   float ow2;              // 2 / dirKnlWidth^2 (Gaussian direction kernels)
   // Distance culling (Gaussian centre kernel only): bounding boxes (lo, hi) of the
   // scaled centres of every 32-element block, deformed (dbb, per EDtot / 32) and
-  // target (tbb, per ETtot / 32).  A staged 32-column sub-tile whose boxes are farther
-  // than kCullR2 (scaled squared distance) from the row tile's box is skipped: its
+  // target (tbb, per ETtot / 32).  A 32-column block whose box is farther than
+  // kCullR2 (scaled squared distance) from the row tile's box is skipped: its
   // centre factors are below 2^-kCullR2 and its direction factors at most 1, so every
   // skipped term is below 2^-64 of its pair weight, far below FP32 resolution of a row
   // sum that holds the row's own term (k = 1).
@@ -471,24 +471,18 @@ struct VarifoldOp {
     bx[0] = fminf(l0.x, l1.x); bx[1] = fminf(l0.y, l1.y); bx[2] = fminf(l0.z, l1.z);
     bx[3] = fmaxf(h0.x, h1.x); bx[4] = fmaxf(h0.y, h1.y); bx[5] = fmaxf(h0.z, h1.z);
   }
-  __device__ __forceinline__ const float4 *col_box(int p, int j) const {
+  // true when every column of the aligned 32-column block sb of pair p's j range
+  // (deformed blocks, then target blocks: Edpad is a multiple of 64) is beyond the
+  // cut-off from the row box rb; an empty box (padding) gives infinite gaps
+  __device__ __forceinline__ bool far(int p, const float *rb, int sb) const {
     const PairDesc &P = pd[p];
-    return j < P.Edpad ? dbb + 2 * ((P.el_off + j) / 32)
-                       : tbb + 2 * ((P.tg_off + j - P.Edpad) / 32);
-  }
-  // true when every column of [j0, j0 + cnt) is beyond the cut-off from the row box
-  __device__ __forceinline__ bool far(int p, const float *rb, int j0, int cnt) const {
-    const float4 *a = col_box(p, j0), *b = col_box(p, j0 + cnt - 1);
-    const float4 la = a[0], ha = a[1], lb = b[0], hb = b[1];
-    const float lo[3] = {fminf(la.x, lb.x), fminf(la.y, lb.y), fminf(la.z, lb.z)};
-    const float hi[3] = {fmaxf(ha.x, hb.x), fmaxf(ha.y, hb.y), fmaxf(ha.z, hb.z)};
-    float d2 = 0.0f;
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const float gap = fmaxf(0.0f, fmaxf(lo[d] - rb[3 + d], rb[d] - hi[d]));
-      d2 = fmaf(gap, gap, d2);
-    }
-    return d2 > kCullR2;  // empty boxes give inf gaps
+    const int db = P.Edpad / 32;
+    const float4 *bx = sb < db ? dbb + 2 * (P.el_off / 32 + sb) : tbb + 2 * (P.tg_off / 32 + sb - db);
+    const float4 lo = bx[0], hi = bx[1];
+    const float gx = fmaxf(0.0f, fmaxf(lo.x - rb[3], rb[0] - hi.x));
+    const float gy = fmaxf(0.0f, fmaxf(lo.y - rb[4], rb[1] - hi.y));
+    const float gz = fmaxf(0.0f, fmaxf(lo.z - rb[5], rb[2] - hi.z));
+    return fmaf(gz, gz, fmaf(gy, gy, gx * gx)) > kCullR2;
   }
 
   __device__ bool active(int p) const { return act[p] != 0; }

@@ -153,26 +153,19 @@ __global__ void __launch_bounds__(W * 32)
   for (int a = 0; a < NA; ++a) hi0[a] = lo0[a] = hi1[a] = lo1[a] = 0.0f;
   const int J = op.j_count(p);
   const int nw = S * W, gw = rank * W + warp;
-  const int jb = (int)((long long)J * gw / nw), je = (int)((long long)J * (gw + 1) / nw);
   const int split = Op::kTwoSets ? op.set_boundary(p) : J;
   float4 nxt[JWP];
-  if (jb + lane < je) op.load_j2(p, jb + lane, nxt);
-  for (int j0 = jb; j0 < je; j0 += kSub) {
+  auto stage = [&]() {  // prefetched registers -> the warp's shared-memory sub-tile
     __syncwarp();
 #pragma unroll
     for (int x = 0; x < JWP; ++x) s_j[warp][x][lane] = nxt[x];
     __syncwarp();
-    const int cnt = min(kSub, je - j0);
-    const int jn = j0 + kSub;
-    if (jn + lane < je) op.load_j2(p, jn + lane, nxt);
+  };
+  auto consume = [&](int j0, int cnt) {  // staged [j0, j0 + cnt) -> TwoSum accumulators
     float2 a[NA];
 #pragma unroll
     for (int k = 0; k < NA; ++k) a[k] = make_float2(0.0f, 0.0f);
-    bool skip = false;  // warp-uniform: the same rows and sub-tile for every lane
-    if constexpr (Op::kCull) skip = op.far(p, s_rbox, j0, cnt);
-    if (skip) {
-      // every term of the sub-tile is below the cut-off: nothing to add
-    } else if (Op::kTwoSets) {
+    if (Op::kTwoSets) {
       const int b = min(max(split - j0, 0), cnt);  // [0, b) first set, [b, cnt) second
       if (b > 0) run_sub2<0>(op, s_j[warp], 0, b, I, a);
       if (b < cnt) run_sub2<1>(op, s_j[warp], b, cnt, I, a);
@@ -183,6 +176,36 @@ __global__ void __launch_bounds__(W * 32)
     for (int k = 0; k < NA; ++k) {
       two_sum_acc(hi0[k], lo0[k], a[k].x);
       two_sum_acc(hi1[k], lo1[k], a[k].y);
+    }
+  };
+  if constexpr (Op::kCull) {
+    // Ops with distance culling: warp gw of the cluster takes the aligned 32-column
+    // sub-tiles gw, gw + nw, gw + 2 nw, ... (J is a multiple of kTile), so the
+    // columns that survive the cut-off, which cluster in index, spread evenly over
+    // the warps; a sub-tile beyond the cut-off is neither loaded nor evaluated.
+    const int nsub = J / kSub;
+    auto next = [&](int s) {  // warp-uniform: the same row box and block for every lane
+      while (s < nsub && op.far(p, s_rbox, s)) s += nw;
+      return s;
+    };
+    int s = next(gw);
+    if (s < nsub) op.load_j2(p, s * kSub + lane, nxt);
+    while (s < nsub) {
+      stage();
+      const int sn = next(s + nw);
+      if (sn < nsub) op.load_j2(p, sn * kSub + lane, nxt);
+      consume(s * kSub, kSub);
+      s = sn;
+    }
+  } else {
+    // every warp of the cluster takes one contiguous, equal (+-1) share of the j range
+    const int jb = (int)((long long)J * gw / nw), je = (int)((long long)J * (gw + 1) / nw);
+    if (jb + lane < je) op.load_j2(p, jb + lane, nxt);
+    for (int j0 = jb; j0 < je; j0 += kSub) {
+      stage();
+      const int jn = j0 + kSub;
+      if (jn + lane < je) op.load_j2(p, jn + lane, nxt);
+      consume(j0, min(kSub, je - j0));
     }
   }
   finish_tile<Op, W>(op, p, tile, rank, S, hi0, lo0, hi1, lo1);

@@ -457,56 +457,6 @@ def run_objgrd(args):
     ctx.close()
 
 
-def _varifold_computed_fraction(P, S, warps=4, tile=64, sub=32):
-    """Share of the varifold sweep's Ed x (Ed + Et) pairs that it evaluates at the
-    source geometry (zero momenta) under its distance culling, by the sweep's own
-    partition and test: 64-row tiles; S x ``warps`` equal contiguous column shares per
-    tile, walked in 32-column sub-tiles; a sub-tile is skipped when the union of the
-    boxes of the (at most two) 32-element column blocks it touches lies farther than
-    squared distance 64 from the row tile's box, in the Gaussian centre kernel's
-    scaled units (k = 2^-|x|^2).  None for a kernel without culling."""
-    import numpy as np
-
-    if P.cen_type != "G":
-        return None
-    s = float(np.float32(np.sqrt(np.log2(np.e)) / P.cen_width))
-    Ed, Et = P.elm_vtx.shape[0], P.tgt_cen.shape[0]
-    Edp, Etp = -(-Ed // tile) * tile, -(-Et // tile) * tile
-    D = P.ini_nde.shape[1]
-
-    def block_boxes(cen, n, npad):
-        c = np.zeros((npad, 3), np.float32)
-        c[:n, :D] = (cen * s).astype(np.float32)
-        real = (np.arange(npad) < n)[:, None]
-        lo = np.where(real, c, np.inf).reshape(-1, 32, 3).min(axis=1)
-        hi = np.where(real, c, -np.inf).reshape(-1, 32, 3).max(axis=1)
-        return lo, hi
-
-    dlo, dhi = block_boxes(P.ini_nde[P.elm_vtx].mean(axis=1), Ed, Edp)
-    tlo, thi = block_boxes(P.tgt_cen, Et, Etp)
-    clo, chi = np.concatenate([dlo, tlo]), np.concatenate([dhi, thi])  # by column // 32
-    J, nw = Edp + Etp, S * warps
-    j0s, cnts = [], []
-    for gw in range(nw):
-        jb, je = J * gw // nw, J * (gw + 1) // nw
-        for j0 in range(jb, je, sub):
-            j0s.append(j0)
-            cnts.append(min(sub, je - j0))
-    j0s, cnts = np.array(j0s), np.array(cnts)
-    b0, b1 = j0s // 32, (j0s + cnts - 1) // 32
-    slo, shi = np.minimum(clo[b0], clo[b1]), np.maximum(chi[b0], chi[b1])
-    rlo = np.minimum(dlo[0::2], dlo[1::2])
-    rhi = np.maximum(dhi[0::2], dhi[1::2])
-    done = 0
-    with np.errstate(invalid="ignore"):
-        for t0 in range(0, rlo.shape[0], 256):
-            a, b = rlo[t0:t0 + 256, None, :], rhi[t0:t0 + 256, None, :]
-            gap = np.maximum(0.0, np.maximum(slo[None] - b, a - shi[None]))
-            keep = (gap * gap).sum(axis=2) <= 64.0
-            done += int((keep * cnts[None]).sum()) * tile
-    return done / (Edp * J)
-
-
 def run_large_pair(args):
     """One large pair: a star-shaped surface on the 7-times subdivided icosphere
     (163,842 landmarks, 327,680 triangles) onto a star-shaped target on the 6-times
@@ -519,7 +469,7 @@ def run_large_pair(args):
     import numpy as np
     import torch
 
-    from lddmm_b200 import _lib, api, problem
+    from lddmm_b200 import _lib, api, culling, problem
 
     itr = args.itr if args.itr != 500 else 100
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -541,7 +491,7 @@ def run_large_pair(args):
                    "frac_of_measured_fp32": tf / peak.value}
     # the varifold sweep skips sub-tiles beyond its centre kernel's cut-off: its
     # roofline counts the pairs it evaluates, its effective rate all of them
-    kept = _varifold_computed_fraction(P, ctx.launch_config()[2])
+    kept = culling.varifold_kept_fraction(P)  # zero momenta: the source geometry
     if kept is not None:
         v = frac["varifold"]
         v["pairs_computed_fraction"] = kept

@@ -961,16 +961,19 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
                      cudaMemcpyHostToDevice, c.stream));
   {
     // bounding boxes of the target blocks' scaled centres (hi + lo), real elements only
-    // (a block of padding gets an empty box; a non-finite centre, the whole space);
-    // constant for the context (the deformed blocks' boxes come with the geometry)
+    // (a block of padding gets an empty box; an element with a non-finite centre,
+    // direction or weight, all of space); constant for the context (the deformed
+    // blocks' boxes come with the geometry)
     std::vector<float4> h_tbb((size_t)std::max(c.ETtot / 32, 1) * 2);
     for (int b = 0; b < c.ETtot / 32; ++b) {
       float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
       for (int k = 32 * b; k < 32 * b + 32; ++k) {
         if (!h_treal[k]) continue;
         const float x[3] = {h_tc[k].x + h_tl[k].x, h_tc[k].y + h_tl[k].y, h_tc[k].z + h_tl[k].z};
+        const bool fin = std::isfinite(x[0]) && std::isfinite(x[1]) && std::isfinite(x[2]) &&
+                         std::isfinite(h_tn[k].x) && std::isfinite(h_tn[k].y) &&
+                         std::isfinite(h_tn[k].z) && std::isfinite(h_tc[k].w);
         for (int d = 0; d < 3; ++d) {
-          const bool fin = std::isfinite(x[d]);
           lo[d] = std::min(lo[d], fin ? x[d] : -INFINITY);
           hi[d] = std::max(hi[d], fin ? x[d] : INFINITY);
         }

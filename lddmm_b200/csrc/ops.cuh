@@ -749,8 +749,12 @@ __device__ __forceinline__ void geometry_element(const PairDesc &P, int4 ev, int
   e[1] = n[1];
   e[2] = n[2];
   e[3] = a;
+  // a non-finite centre, normal or weight makes every pair of the element non-finite
+  // in the all-pairs sums: flagged by a NaN centre, so that its block is never culled
+  const bool fin = isfinite(c[0] * s) && isfinite(c[1] * s) && isfinite(c[2] * s) &&
+                   isfinite(n[0]) && isfinite(n[1]) && isfinite(n[2]) && isfinite(a);
 #pragma unroll
-  for (int d = 0; d < 3; ++d) cf[d] = hi[d] + lo[d];
+  for (int d = 0; d < 3; ++d) cf[d] = fin ? hi[d] + lo[d] : NAN;
 }
 
 template <int D>
@@ -767,13 +771,13 @@ __global__ void geometry_kernel(const PairDesc *__restrict__ pd, const int *__re
   if (live) geometry_element<D>(pd[ev.w], ev, g, q64, ec, en, el, e64, cf);
   // bounding box of the scaled centres of the warp's 32 elements (one block of one
   // pair: pairs are padded to multiples of 64), for the varifold sweep's distance test.
-  // A block of padding gets an empty box; a non-finite centre widens the box to the
-  // whole space, so that no sub-tile holding it is ever skipped.
+  // A block of padding gets an empty box; an element flagged non-finite widens the box
+  // to all of space, so that no block holding it is ever skipped.
   if (bbox && (g - threadIdx.x % 32) < n_elm) {
+    const bool fin = isfinite(cf[0]) && isfinite(cf[1]) && isfinite(cf[2]);
     float lo[3], hi[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const bool fin = isfinite(cf[d]);
       lo[d] = live ? (fin ? cf[d] : -INFINITY) : INFINITY;
       hi[d] = live ? (fin ? cf[d] : INFINITY) : -INFINITY;
 #pragma unroll

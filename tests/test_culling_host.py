@@ -1,0 +1,39 @@
+"""Host restatement of the varifold sweep's culling test (no GPU): which
+(64-row tile, 32-column block) pairs survive the 2^-64 cut-off."""
+import numpy as np
+
+from lddmm_b200 import culling, problem
+
+
+def test_wide_kernel_keeps_every_pair():
+    P = problem.sphere_to_cube(subdiv=2, cube_n=6, time_num=3, sigma_w=10.0)
+    assert culling.varifold_kept_fraction(P) == 1.0
+
+
+def test_cauchy_kernel_has_no_culling():
+    P = problem.sphere_to_cube(subdiv=2, cube_n=6, time_num=3)
+    P.cen_type = "C"
+    assert culling.varifold_kept_fraction(P) is None
+
+
+def test_far_target_keeps_only_deformed_blocks():
+    P = problem.sphere_to_cube(subdiv=2, cube_n=6, time_num=3, sigma_w=10.0)
+    P.tgt_cen = P.tgt_cen + np.array([1e4, 0.0, 0.0])
+    Ed, Et = P.elm_vtx.shape[0], P.tgt_cen.shape[0]
+    pad = lambda n: -(-n // 64) * 64
+    assert culling.varifold_kept_fraction(P) == pad(Ed) / (pad(Ed) + pad(Et))
+
+
+def test_nonfinite_centre_widens_its_block():
+    P = problem.sphere_to_cube(subdiv=2, cube_n=6, time_num=3, sigma_w=10.0)
+    P.tgt_cen = P.tgt_cen + np.array([1e4, 0.0, 0.0])
+    base = culling.varifold_kept_fraction(P)
+    t = P.tgt_cen.copy()
+    t[0, 1] = np.nan
+    P.tgt_cen = t
+    # the first target block now meets every row tile
+    rows = -(-P.elm_vtx.shape[0] // 64)
+    Ed, Et = P.elm_vtx.shape[0], P.tgt_cen.shape[0]
+    pad = lambda n: -(-n // 64) * 64
+    extra = rows * 64 * 32 / (pad(Ed) * (pad(Ed) + pad(Et)))
+    assert abs(culling.varifold_kept_fraction(P) - (base + extra)) < 1e-12

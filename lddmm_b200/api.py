@@ -275,6 +275,38 @@ def computeNodePosition(iniNdeMat, alpStk, knlOrder, knlWidth, timeStp, timeNum)
     return np.transpose(nde, (2, 1, 0)), np.transpose(vlc, (2, 1, 0))
 
 
+def _scalar(v):
+    """A MATLAB scalar or char array as loaded from a .mat file (1 x 1 arrays, 1-element
+    string arrays) or as given in Python."""
+    a = np.asarray(v)
+    if a.dtype.kind in "US":
+        return str(a.ravel()[0]) if a.size else ""
+    return a.ravel()[0].item() if a.size == 1 else v
+
+
+def problem_from_matlab(iniNdeMat, disObj, knlOrder, knlWidth, timeEnd, timeStp) -> Problem:
+    """The problem that ``LDDMM`` (Cpp/src/LDDMM.m) solves, from its MATLAB-layout
+    arguments: iniNdeMat dim x N; disObj (dict or object) with dfmElmVtxMat
+    ((2|3) x E_d, 1-based), tgtCenPosMat / tgtUniDirMat (dim x E_t), tgtElmVolVec
+    (E_t values), cenKnlType, cenKnlWidth, dirKnlType, dirKnlWidth, disWgt; timeNum =
+    floor(timeEnd / timeStp) + 1.  Fields may be numpy values or the 1 x 1 arrays that
+    ``scipy.io.loadmat`` returns."""
+    d = disObj if isinstance(disObj, dict) else vars(disObj)
+    ini = np.asarray(iniNdeMat, dtype=np.float64)
+    timeEnd, timeStp = float(_scalar(timeEnd)), float(_scalar(timeStp))
+    timeNum = int(math.floor(timeEnd / timeStp)) + 1
+    ev = np.asarray(d["dfmElmVtxMat"]).T.astype(np.int32) - 1
+    return Problem(ini.T, ev, np.asarray(d["tgtCenPosMat"], dtype=np.float64).T,
+                   np.asarray(d["tgtUniDirMat"], dtype=np.float64).T,
+                   np.asarray(d["tgtElmVolVec"], dtype=np.float64).ravel(),
+                   knl_order=int(_scalar(knlOrder)), knl_width=float(_scalar(knlWidth)),
+                   time_num=timeNum, time_stp=timeStp, cen_type=str(_scalar(d["cenKnlType"])),
+                   cen_width=float(_scalar(d["cenKnlWidth"])),
+                   dir_type=str(_scalar(d["dirKnlType"])),
+                   dir_width=float(_scalar(d["dirKnlWidth"])),
+                   dis_wgt=float(_scalar(d["disWgt"])))
+
+
 def LDDMM(iniNdeMat, iniAlpStk, disObj, knlOrder, knlWidth, timeEnd, timeStp, optObj):
     """``Cpp/src/LDDMM.m``: [ndeStk, vlcStk, alpStk] = LDDMM(iniNdeMat, iniAlpStk,
     disObj, knlOrder, knlWidth, timeEnd, timeStp, optObj).
@@ -284,19 +316,11 @@ def LDDMM(iniNdeMat, iniAlpStk, disObj, knlOrder, knlWidth, timeEnd, timeStp, op
     dirKnlType, dirKnlWidth, disWgt; optObj has MaxIterations, OptimalityTolerance,
     Wolfe1, Wolfe2, Columns, Verbose.  Missing optObj fields take the defaults of
     MATLAB/src/LBFGS.m:86-110.  iniAlpStk may be None (zeros)."""
-    d = disObj if isinstance(disObj, dict) else vars(disObj)
     o = optObj if isinstance(optObj, dict) else vars(optObj)
     ini = np.asarray(iniNdeMat, dtype=np.float64)
     dim, n = ini.shape
-    timeNum = int(math.floor(timeEnd / timeStp)) + 1
-    ev = np.asarray(d["dfmElmVtxMat"]).T.astype(np.int32) - 1
-    P = Problem(ini.T, ev, np.asarray(d["tgtCenPosMat"], dtype=np.float64).T,
-                np.asarray(d["tgtUniDirMat"], dtype=np.float64).T,
-                np.asarray(d["tgtElmVolVec"], dtype=np.float64).ravel(),
-                knl_order=int(knlOrder), knl_width=float(knlWidth), time_num=timeNum,
-                time_stp=float(timeStp), cen_type=str(d["cenKnlType"]),
-                cen_width=float(d["cenKnlWidth"]), dir_type=str(d["dirKnlType"]),
-                dir_width=float(d["dirKnlWidth"]), dis_wgt=float(d["disWgt"]))
+    P = problem_from_matlab(iniNdeMat, disObj, knlOrder, knlWidth, timeEnd, timeStp)
+    timeNum = P.time_num
     nvar = dim * n * (timeNum - 1)
     if iniAlpStk is None or np.size(iniAlpStk) == 0:
         alp0 = np.zeros(nvar)
@@ -304,12 +328,13 @@ def LDDMM(iniNdeMat, iniAlpStk, disObj, knlOrder, knlWidth, timeEnd, timeStp, op
         alp0 = np.transpose(np.asarray(iniAlpStk, dtype=np.float64).reshape(
             dim, n, timeNum - 1, order="F"), (2, 1, 0)).reshape(-1)
     with Context(P) as ctx:
-        x, res = ctx.lbfgs(alp0, itr_max=int(o.get("MaxIterations", 1000)),
-                           tol=float(o.get("OptimalityTolerance", 1e-6)),
-                           wolfe1=float(o.get("Wolfe1", 1e-4)),
-                           wolfe2=float(o.get("Wolfe2", 0.9)),
-                           mem_num=int(min(o.get("Columns", min(100, nvar)), 32)),
-                           verbose=bool(o.get("Verbose", False)))
+        x, res = ctx.lbfgs(alp0, itr_max=int(_scalar(o.get("MaxIterations", 1000))),
+                           tol=float(_scalar(o.get("OptimalityTolerance", 1e-6))),
+                           wolfe1=float(_scalar(o.get("Wolfe1", 1e-4))),
+                           wolfe2=float(_scalar(o.get("Wolfe2", 0.9))),
+                           mem_num=int(min(_scalar(o.get("Columns", min(100, nvar))), 32)),
+                           verbose=bool(_scalar(o.get("Verbose", False))))
     alpStk = np.transpose(x.reshape(timeNum - 1, n, dim), (2, 1, 0))
-    ndeStk, vlcStk = computeNodePosition(ini, alpStk, knlOrder, knlWidth, timeStp, timeNum)
+    ndeStk, vlcStk = computeNodePosition(ini, alpStk, P.knl_order, P.knl_width, P.time_stp,
+                                         timeNum)
     return SimpleNamespace(ndeStk=ndeStk, vlcStk=vlcStk, alpStk=alpStk, result=res[0])

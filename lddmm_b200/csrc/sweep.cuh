@@ -182,17 +182,29 @@ __global__ void __launch_bounds__(W * 32)
     // Ops with distance culling: warp gw of the cluster takes the aligned 32-column
     // sub-tiles gw, gw + nw, gw + 2 nw, ... (J is a multiple of kTile), so the
     // columns that survive the cut-off, which cluster in index, spread evenly over
-    // the warps; a sub-tile beyond the cut-off is neither loaded nor evaluated.
+    // the warps; a sub-tile beyond the cut-off is neither loaded nor evaluated.  The
+    // cut-off test runs for 32 candidates at once (lane l tests candidate base + l nw)
+    // and a ballot keeps the survivors, so the box loads cost one round trip per 32
+    // candidates instead of one per skipped sub-tile.
     const int nsub = J / kSub;
-    auto next = [&](int s) {  // warp-uniform: the same row box and block for every lane
-      while (s < nsub && op.far(p, s_rbox, s)) s += nw;
-      return s;
+    int base = gw - 32 * nw;  // first candidate of the current group
+    unsigned mask = 0u;       // survivors of the current group not yet taken
+    auto next = [&]() {       // warp-uniform: the next surviving sub-tile, or nsub
+      while (mask == 0u) {
+        base += 32 * nw;
+        if (base >= nsub) return nsub;
+        const int sb = base + lane * nw;
+        mask = __ballot_sync(0xffffffffu, sb < nsub && !op.far(p, s_rbox, sb));
+      }
+      const int k = __ffs(mask) - 1;
+      mask &= mask - 1u;
+      return base + k * nw;
     };
-    int s = next(gw);
+    int s = next();
     if (s < nsub) op.load_j2(p, s * kSub + lane, nxt);
     while (s < nsub) {
       stage();
-      const int sn = next(s + nw);
+      const int sn = next();
       if (sn < nsub) op.load_j2(p, sn * kSub + lane, nxt);
       consume(s * kSub, kSub);
       s = sn;

@@ -345,6 +345,8 @@ def run_ours(args):
                    "varifold": sweeps["varifold"]}
     dom = max(per_eval_ms, key=per_eval_ms.get)
     achieved = pairs_launch[dom] * fl[dom] / (sweeps[dom] * 1e-3) / 1e12
+    pipes = _pipe_peaks(local)
+    mufu = _mufu_frac(dom, P, pairs_launch[dom], sweeps[dom], pipes)
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as fh:
@@ -403,7 +405,8 @@ def run_ours(args):
                          "peak": peak.value, "unit": "TFLOP/s", "frac": achieved / peak.value,
                          "peak_source": "measured FP32 FMA probe (lddmm_fp32_peak), same GPU",
                          "flops_per_pair": fl[dom], "pairs_per_launch": pairs_launch[dom],
-                         "traffic": traffic},
+                         "traffic": traffic, "fp32x2_peak_tflops": pipes["fp32x2_tflops"],
+                         "mufu": mufu},
             "cpu_baseline": cpu,
             "e2e": {"value": replicas.job_rate(e_steps, world, e_ms * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -457,6 +460,36 @@ def run_objgrd(args):
     ctx.close()
 
 
+def _pipe_peaks(device):
+    """Probe-measured throughput of the pipes the sweeps use (lddmm_pipe_peaks)."""
+    import ctypes as C
+
+    from lddmm_b200 import _lib
+
+    out = (C.c_double * 3)()
+    _lib.check(_lib.lib.lddmm_pipe_peaks(device, out))
+    return {"fp32_tflops": out[0], "fp32x2_tflops": out[1], "ex2_gops": out[2]}
+
+
+def _mufu_per_pair(sweep, P):
+    """MUFU operations per pair as the sweeps execute them: a Gaussian deformation
+    kernel one ex2, a 3D Matern kernel a square root and an ex2; the varifold's
+    Gaussian centre kernel one ex2 (Cauchy: one reciprocal), plus one ex2 for the
+    'O' / 'U' direction kernels ('B' and 'L' none)."""
+    if sweep in ("shoot", "adjoint"):
+        return 1 if P.knl_order == -1 else 2
+    return 1 + (1 if P.dir_type in ("O", "U") else 0)
+
+
+def _mufu_frac(sweep, P, pairs, ms, pipes):
+    """The sweep's MUFU rate against the probe's ex2 rate: the second ceiling of an
+    all-pairs sweep next to the FP32 FMA one."""
+    m = _mufu_per_pair(sweep, P)
+    g = pairs * m / (ms * 1e-3) / 1e9
+    return {"ops_per_pair": m, "achieved_gops": g, "peak_gops": pipes["ex2_gops"],
+            "frac": g / pipes["ex2_gops"]}
+
+
 def run_large_pair(args):
     """One large pair: a star-shaped surface on the 7-times subdivided icosphere
     (163,842 landmarks, 327,680 triangles) onto a star-shaped target on the 6-times
@@ -498,6 +531,10 @@ def run_large_pair(args):
         v["tflops_effective"] = v["tflops"]
         v["tflops"] *= kept
         v["frac_of_measured_fp32"] *= kept
+    pipes = _pipe_peaks(local)
+    for k in frac:
+        evaluated = pairs_launch[k] * (frac[k].get("pairs_computed_fraction") or 1.0)
+        frac[k]["mufu"] = _mufu_frac(k, P, evaluated, sweeps[k], pipes)
     x0 = np.zeros(ctx.var_total)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -515,7 +552,8 @@ def run_large_pair(args):
         "status": r["status"], "f": r["f"], "seconds": s,
         "ms_per_evaluation": s * 1e3 / max(r["evals"], 1),
         "gpair_interactions_per_s": (r["evals"] * pairs_eval + Et * Et) / s / 1e9,
-        "sweeps": frac, "fp32_peak_tflops": peak.value, "clocks": clk.summary()}),
+        "sweeps": frac, "fp32_peak_tflops": peak.value, "pipe_peaks": pipes,
+        "clocks": clk.summary()}),
         flush=True)
     ctx.close()
 

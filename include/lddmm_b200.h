@@ -271,6 +271,12 @@ int lddmm_wait_selftest(int device, int never_released, double *ms);
  * FP32-bound sweeps.  Returns 0 and writes the figure to *tflops. */
 int lddmm_fp32_peak(int device, double *tflops);
 
+/* Throughput of the pipes the all-pairs sweeps use, measured on `device` by probe
+ * kernels (best of three launches): out[0] scalar FP32 FMA TFLOP/s (as
+ * lddmm_fp32_peak), out[1] packed FP32x2 FMA TFLOP/s, out[2] ex2.approx (MUFU)
+ * results per second, in G/s.  The rooflines of the sweeps are read against these. */
+int lddmm_pipe_peaks(int device, double *out);
+
 /* FLOPs per pair interaction the roofline uses (FMA = 2, as executed), for the
  * shooting step, the fused adjoint step and the varifold pair of the given kinds. */
 double lddmm_flops_per_pair(int sweep, int dim, int knl_order, char cen_type, char dir_type);

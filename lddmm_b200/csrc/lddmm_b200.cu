@@ -2385,6 +2385,80 @@ extern "C" int lddmm_fp32_peak(int device, double *tflops) {
   return 0;
 }
 
+// Packed form of the probe: 4 independent FP32x2 chains (8 FMAs per iteration, as
+// above) through the sm_100 paired FMA.
+__global__ void fp32x2_probe_kernel(float *out, int iters, float seed) {
+  float2 a[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    a[k] = make_float2(seed + threadIdx.x * 1e-6f + k, seed + threadIdx.x * 1e-6f + k + 0.5f);
+  const float2 m = make_float2(0.999999f, 0.999999f), c = make_float2(1e-7f, 1e-7f);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) a[k] = __ffma2_rn(a[k], m, c);
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s += a[k].x + a[k].y;
+  if (s == -12345.0f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// MUFU probe: 8 independent chains x <- 2^-x per thread (the ex2.approx the all-pairs
+// loops use; the values stay in [0.5, 1]).
+__global__ void ex2_probe_kernel(float *out, int iters, float seed) {
+  float a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = seed * 1e-3f + threadIdx.x * 1e-7f + 0.1f * k;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = ex2f(-a[k]);
+  }
+  float s = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += a[k];
+  if (s == -12345.0f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// Per-pipe throughput on `device`: out[0] scalar FP32 FMA TFLOP/s (the probe of
+// lddmm_fp32_peak), out[1] packed FP32x2 FMA TFLOP/s, out[2] ex2.approx Gop/s
+// (MUFU).  Best of three timed launches after a warm-up launch each.
+extern "C" int lddmm_pipe_peaks(int device, double *out) {
+  if (!out) return LDDMM_ERR_ARG;
+  CU(cudaSetDevice(device));
+  int sms = 0;
+  CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  const int threads = 256, blocks = sms * 8;
+  float *buf = nullptr;
+  CU(cudaMalloc(&buf, sizeof(float) * threads * blocks));
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  cudaError_t err = cudaSuccess;
+  for (int which = 0; which < 3 && err == cudaSuccess; ++which) {
+    const int iters = which == 2 ? 1 << 13 : 1 << 15;
+    float best = 1e30f;
+    for (int rep = 0; rep < 4 && err == cudaSuccess; ++rep) {
+      cudaEventRecord(e0);
+      if (which == 0) fp32_probe_kernel<<<blocks, threads>>>(buf, iters, 1.0f);
+      else if (which == 1) fp32x2_probe_kernel<<<blocks, threads>>>(buf, iters, 1.0f);
+      else ex2_probe_kernel<<<blocks, threads>>>(buf, iters, 1.0f);
+      cudaEventRecord(e1);
+      err = cudaGetLastError();
+      if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+      float ms = 0.0f;
+      if (err == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0) best = std::min(best, ms);
+    }
+    const double ops = 8.0 * iters * (double)threads * blocks;
+    out[which] = which == 2 ? ops / (best * 1e-3) / 1e9 : 2.0 * ops / (best * 1e-3) / 1e12;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(buf);
+  CU(err);
+  return 0;
+}
+
 // ================================================================ misc
 
 // ============================================================ wait self-test

@@ -5,7 +5,8 @@
 //             largest pairs first.
 //   cluster = S CTAs on one item (thread-block cluster along x); the S x W warps of
 //             the cluster split the item's j range into contiguous shares that differ
-//             by at most one point.
+//             by at most one point (ops with distance culling: aligned 32-point
+//             blocks dealt to the warps in turn, see sweep_packed_kernel).
 //   CTA     = W warps; every warp owns all 64 rows of the tile (2 rows per lane) and
 //             walks its share in 32-point sub-tiles, staged warp-privately in shared
 //             memory with the next sub-tile prefetched into registers, so warps never
@@ -37,6 +38,9 @@
 //                      (v, v), so both halves of a packed operand come from one
 //                      shared-memory load; the two rows' registers, (row0, row1)
 //   load_i2(p, r0, r1, I), load_j2(p, j, w), pair2<SET>(I, w, acc)  with float2 acc
+//   kCull              skip j blocks beyond a cut-off, given
+//   row_box(p, tile, b) the tile's bounding box (lo[3], hi[3]) in shared memory
+//   far(p, b, block)   the aligned 32-point block lies beyond the cut-off from b
 // Each packed operation applies to each row exactly the scalar operation of pair()
 // in the same order, so both kernels give bitwise the same sums.
 #pragma once

@@ -135,6 +135,7 @@ struct lddmm_ctx {
       nchunk_tot = 0;
   long long nvar = 0;
   int n_pt_items = 0, n_el_items = 0;
+  int n_pt_items2 = 0;  // two-tile items of the per-step shooting sweep
   int S_shoot = 1, S_adj = 1, S_vfd = 1;
   // persistent multi-step sweeps (one cooperative launch per direction)
   bool persistent = false;
@@ -165,6 +166,7 @@ struct lddmm_ctx {
   int4 *adj = nullptr;
   double *reg_part = nullptr, *vfd_part = nullptr, *f_dev = nullptr;
   int2 *pt_items = nullptr, *el_items = nullptr;
+  int2 *pt_items2 = nullptr;  // (pair, even tile): tiles tile and tile + 1 when present
   int *chunk_pair = nullptr;
   double *X = nullptr, *G = nullptr, *XT = nullptr, *GT = nullptr, *Dv = nullptr;
   double *Sh = nullptr, *Yh = nullptr;
@@ -217,7 +219,7 @@ lddmm_ctx::~lddmm_ctx() {
   dfree(el, stream); dfree(tc, stream); dfree(tn, stream); dfree(tl, stream);
   dfree(e64, stream); dfree(dcdd, stream); dfree(tgt64, stream); dfree(elm, stream);
   dfree(pt_pair, stream); dfree(adj_ptr, stream); dfree(adj, stream); dfree(reg_part, stream);
-  dfree(vfd_part, stream); dfree(f_dev, stream); dfree(pt_items, stream);
+  dfree(vfd_part, stream); dfree(f_dev, stream); dfree(pt_items, stream); dfree(pt_items2, stream);
   dfree(el_items, stream); dfree(chunk_pair, stream); dfree(X, stream); dfree(G, stream);
   dfree(XT, stream); dfree(GT, stream); dfree(Dv, stream);
   dfree(Sh, stream); dfree(Yh, stream); dfree(part, stream);
@@ -280,10 +282,19 @@ static cudaError_t shoot_impl(lddmm_ctx &c, int t, double *vlc) {
   op.vlc64 = vlc;
   op.tile_part = c.reg_part + (size_t)t * c.ntile_tot;
   op.t = t;
-  // packed FP32x2 form of the same sweep (bitwise the same sums)
-  return launch(sweep_packed_kernel<ShootOp<D, ORDER>, kWarps>,
-                (unsigned)(c.n_pt_items * c.S_shoot), kWarps * 32, c.S_shoot, c.stream, op,
-                (const int2 *)c.pt_items, c.S_shoot);
+  // packed FP32x2 form of the same sweep (bitwise the same sums).  The Gaussian kernel
+  // runs on two-tile items, each staged column serving four rows per lane: its sweep
+  // is held first by the shared-memory reads (163,842 landmarks: 11.13 -> 10.58 ms);
+  // the Matern kernels, with a square root per pair and fewer CTAs per SM at the
+  // larger register count, are faster on single tiles (40,962: 1.02 vs 1.10 ms).
+  if constexpr (ORDER == -1)
+    return launch(sweep_packed_kernel<ShootOp<D, ORDER>, kWarps, 2>,
+                  (unsigned)(c.n_pt_items2 * c.S_shoot), kWarps * 32, c.S_shoot, c.stream, op,
+                  (const int2 *)c.pt_items2, c.S_shoot);
+  else
+    return launch(sweep_packed_kernel<ShootOp<D, ORDER>, kWarps>,
+                  (unsigned)(c.n_pt_items * c.S_shoot), kWarps * 32, c.S_shoot, c.stream, op,
+                  (const int2 *)c.pt_items, c.S_shoot);
 }
 
 template <int D, int ORDER>
@@ -791,15 +802,18 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   for (int p = 0; p < num; ++p) order[p] = p;
   std::stable_sort(order.begin(), order.end(),
                    [&](int a, int b) { return c.hpd[a].Npad > c.hpd[b].Npad; });
-  std::vector<int2> pti, eli;
+  std::vector<int2> pti, eli, pti2;
   for (int p : order)
     for (int k = 0; k < c.hpd[p].Npad / kTile; ++k) pti.push_back(make_int2(p, k));
+  for (int p : order)
+    for (int k = 0; k < c.hpd[p].Npad / kTile; k += 2) pti2.push_back(make_int2(p, k));
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
     return c.hpd[a].Edpad + c.hpd[a].Etpad > c.hpd[b].Edpad + c.hpd[b].Etpad;
   });
   for (int p : order)
     for (int k = 0; k < c.hpd[p].Edpad / kTile; ++k) eli.push_back(make_int2(p, k));
   c.n_pt_items = (int)pti.size();
+  c.n_pt_items2 = (int)pti2.size();
   c.n_el_items = (int)eli.size();
   std::vector<int2> uni;
   for (const int2 &x : pti)
@@ -939,6 +953,7 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
   CU(dalloc(c.stream, &c.vfd_part, std::max(c.netile_tot, 1)));
   CU(dalloc(c.stream, &c.f_dev, num));
   CU(dalloc(c.stream, &c.pt_items, std::max(c.n_pt_items, 1)));
+  CU(dalloc(c.stream, &c.pt_items2, std::max(c.n_pt_items2, 1)));
   CU(dalloc(c.stream, &c.el_items, std::max(c.n_el_items, 1)));
   CU(dalloc(c.stream, &c.chunk_pair, c.nchunk_tot));
   CU(dalloc(c.stream, &c.XT, c.nvar));
@@ -994,6 +1009,9 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
                        cudaMemcpyHostToDevice, c.stream));
   if (c.n_pt_items)
     CU(cudaMemcpyAsync(c.pt_items, pti.data(), sizeof(int2) * pti.size(),
+                       cudaMemcpyHostToDevice, c.stream));
+  if (c.n_pt_items2)
+    CU(cudaMemcpyAsync(c.pt_items2, pti2.data(), sizeof(int2) * pti2.size(),
                        cudaMemcpyHostToDevice, c.stream));
   if (c.n_el_items)
     CU(cudaMemcpyAsync(c.el_items, eli.data(), sizeof(int2) * eli.size(),

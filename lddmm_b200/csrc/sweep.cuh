@@ -131,7 +131,29 @@ __device__ __forceinline__ void run_sub2(const Op &op, const float4 (*sj)[kSub],
   }
 }
 
-template <class Op, int W>
+// Two row tiles against one staged sub-tile: each column is read from shared memory
+// once for the lane's four rows (the same operations per row as run_sub2).
+template <int SET, class Op>
+__device__ __forceinline__ void run_sub2x2(const Op &op, const float4 (*sj)[kSub], int lo,
+                                           int hi, const typename Op::IData2 &I,
+                                           const typename Op::IData2 &Ib, float2 (&a)[Op::NA],
+                                           float2 (&b)[Op::NA]) {
+#pragma unroll 4
+  for (int jj = lo; jj < hi; ++jj) {
+    float4 w[Op::JWP];
+#pragma unroll
+    for (int x = 0; x < Op::JWP; ++x) w[x] = sj[x][jj];
+    op.template pair2<SET>(I, w, a);
+    op.template pair2<SET>(Ib, w, b);
+  }
+}
+
+// TPW (tiles per work item) = 2: an item is row tiles `tile` and `tile + 1` of one
+// pair (the second only when the pair has it, Op::i_count), so that every staged
+// column serves four rows per lane and the shared-memory reads per pair halve.  Each
+// row sees the same column shares in the same order as with TPW = 1, so the sums are
+// bitwise the same.
+template <class Op, int W, int TPW = 1>
 __global__ void __launch_bounds__(W * 32)
     sweep_packed_kernel(const Op op, const int2 *__restrict__ items, int S) {
   constexpr int JWP = Op::JWP;
@@ -150,11 +172,17 @@ __global__ void __launch_bounds__(W * 32)
     if (threadIdx.x == 0) op.row_box(p, tile, s_rbox);
     __syncthreads();
   }
-  typename Op::IData2 I;
+  typename Op::IData2 I, Ib;
   op.load_i2(p, tile * kTile + lane, tile * kTile + 32 + lane, I);
-  float hi0[NA], lo0[NA], hi1[NA], lo1[NA];
+  bool two = false;  // uniform over the cluster: a second row tile in this item
+  if constexpr (TPW == 2) {
+    two = (tile + 1) * kTile < op.i_count(p);
+    if (two) op.load_i2(p, (tile + 1) * kTile + lane, (tile + 1) * kTile + 32 + lane, Ib);
+  }
+  float hi0[NA], lo0[NA], hi1[NA], lo1[NA], hi2[NA], lo2[NA], hi3[NA], lo3[NA];
 #pragma unroll
-  for (int a = 0; a < NA; ++a) hi0[a] = lo0[a] = hi1[a] = lo1[a] = 0.0f;
+  for (int a = 0; a < NA; ++a)
+    hi0[a] = lo0[a] = hi1[a] = lo1[a] = hi2[a] = lo2[a] = hi3[a] = lo3[a] = 0.0f;
   const int J = op.j_count(p);
   const int nw = S * W, gw = rank * W + warp;
   const int split = Op::kTwoSets ? op.set_boundary(p) : J;
@@ -169,7 +197,22 @@ __global__ void __launch_bounds__(W * 32)
     float2 a[NA];
 #pragma unroll
     for (int k = 0; k < NA; ++k) a[k] = make_float2(0.0f, 0.0f);
-    if (Op::kTwoSets) {
+    if constexpr (TPW == 2) {
+      static_assert(!Op::kTwoSets, "two-tile items serve one-set sweeps");
+      if (two) {
+        float2 b[NA];
+#pragma unroll
+        for (int k = 0; k < NA; ++k) b[k] = make_float2(0.0f, 0.0f);
+        run_sub2x2<0>(op, s_j[warp], 0, cnt, I, Ib, a, b);
+#pragma unroll
+        for (int k = 0; k < NA; ++k) {
+          two_sum_acc(hi2[k], lo2[k], b[k].x);
+          two_sum_acc(hi3[k], lo3[k], b[k].y);
+        }
+      } else {
+        run_sub2<0>(op, s_j[warp], 0, cnt, I, a);
+      }
+    } else if (Op::kTwoSets) {
       const int b = min(max(split - j0, 0), cnt);  // [0, b) first set, [b, cnt) second
       if (b > 0) run_sub2<0>(op, s_j[warp], 0, b, I, a);
       if (b < cnt) run_sub2<1>(op, s_j[warp], b, cnt, I, a);
@@ -225,6 +268,12 @@ __global__ void __launch_bounds__(W * 32)
     }
   }
   finish_tile<Op, W>(op, p, tile, rank, S, hi0, lo0, hi1, lo1);
+  if constexpr (TPW == 2) {
+    if (two) {
+      __syncthreads();  // the first tile's reduction is done with the shared arrays
+      finish_tile<Op, W>(op, p, tile + 1, rank, S, hi2, lo2, hi3, lo3);
+    }
+  }
 }
 
 template <class Op, int W>

@@ -206,3 +206,24 @@ def test_shoot_trajectory(api, oracle):
                                 P.time_num)
     assert mrel(nde, nde_o) < TOL
     assert mrel(vlc, vlc_o) < TOL
+
+
+def test_two_tile_gaussian_shoot_odd_tiles_vs_oracle(api, oracle):
+    """Per-step sweeps with the Gaussian kernel: the shooting sweep runs on two-tile
+    items, and 642 landmarks give 11 tiles, so the last item holds one tile only.
+    Objective and gradient against the FP64 oracle, and the persistent time-loop
+    sweeps (single tiles) within the same tolerance."""
+    from lddmm_b200 import problem
+
+    P = problem.sphere_to_cube(subdiv=3, cube_n=10, time_num=6, knl_order=-1, knl_width=0.3)
+    assert (-(-P.nde_num // 64)) % 2 == 1
+    alp = np.random.default_rng(21).normal(size=P.var_num) * 0.05
+    with api.Context(P, persistent=-1) as ctx:
+        f, g = ctx.objgrd(alp)
+    with api.Context(P, persistent=1) as ctx:
+        f1, g1 = ctx.objgrd(alp)
+    fo, go = oracle.objgrd(P, alp)
+    assert abs(f[0] - fo) / abs(fo) < TOL
+    assert rel(g, go) < TOL
+    assert abs(f1[0] - fo) / abs(fo) < TOL
+    assert rel(g1, go) < TOL

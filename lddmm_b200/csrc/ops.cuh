@@ -459,10 +459,13 @@ struct VarifoldOp {
   // Distance culling (Gaussian centre kernel only): bounding boxes (lo, hi) of the
   // scaled centres of every 32-element block, deformed (dbb, per EDtot / 32) and
   // target (tbb, per ETtot / 32).  A 32-column block whose box is farther than
-  // kCullR2 (scaled squared distance) from the row tile's box is skipped: its
-  // centre factors are below 2^-kCullR2 and its direction factors at most 1, so every
-  // skipped term is below 2^-64 of its pair weight, far below FP32 resolution of a row
-  // sum that holds the row's own term (k = 1).
+  // kCullR2 (scaled squared distance x^2) from the row tile's box is skipped: there
+  // k = 2^-x^2 < 2^-64 and its derivative factor x 2^-x^2 <= 8 2^-64, while every
+  // direction factor is at most 1 in magnitude.  Each skipped value term is thus below
+  // 2^-64 of its pair weight (the product of the two areas) and each skipped gradient
+  // term below 2^-61 of its pair weight times the kernel's derivative scale, far
+  // below the FP32 resolution of the varifold value (whose deformed-deformed part
+  // holds every element's own term, k = 1) and of its gradient.
   const float4 *dbb, *tbb;
   static constexpr bool kCull = (CT == 'G');
   static constexpr float kCullR2 = 64.0f;

@@ -314,9 +314,14 @@ static cudaError_t adjoint_impl(lddmm_ctx &c, int t, double *g, double *pdot) {
   op.pdot64 = pdot;
   op.t = t;
   // packed FP32x2 form of the same sweep (bitwise the same sums)
-  return launch(sweep_packed_kernel<AdjointOp<D, ORDER>, kWarps>,
-                (unsigned)(c.n_pt_items * c.S_adj), kWarps * 32, c.S_adj, c.stream, op,
-                (const int2 *)c.pt_items, c.S_adj);
+  if constexpr (ORDER == -1)
+    return launch(sweep_packed_kernel<AdjointOp<D, ORDER>, kWarps, 2>,
+                  (unsigned)(c.n_pt_items2 * c.S_adj), kWarps * 32, c.S_adj, c.stream, op,
+                  (const int2 *)c.pt_items2, c.S_adj);
+  else
+    return launch(sweep_packed_kernel<AdjointOp<D, ORDER>, kWarps>,
+                  (unsigned)(c.n_pt_items * c.S_adj), kWarps * 32, c.S_adj, c.stream, op,
+                  (const int2 *)c.pt_items, c.S_adj);
 }
 
 // Cooperative launch of a persistent multi-step sweep (all CTAs co-resident; the

@@ -230,6 +230,7 @@ struct AdjointOp {
 
   __device__ bool active(int p) const { return act[p] != 0; }
   __device__ int j_count(int p) const { return pd[p].Npad; }
+  __device__ int i_count(int p) const { return pd[p].Npad; }  // rows (two-tile items)
   __device__ int set_boundary(int p) const { return pd[p].Npad; }
   __device__ void load_i(int p, int row, IData &I) const {
     const int g = pd[p].pt_off + row;

@@ -277,6 +277,13 @@ int lddmm_fp32_peak(int device, double *tflops);
  * results per second, in G/s.  The rooflines of the sweeps are read against these. */
 int lddmm_pipe_peaks(int device, double *out);
 
+/* Storage order that lddmm_ctx_create gives the elements of a 3D surface (and the
+ * target's): cen is n x 3 element centres; perm[k] receives the element stored in
+ * slot k.  Returns 1 when the elements are reordered along a Morton curve of their
+ * centres (because that makes the varifold sweep's 32-element blocks more compact),
+ * 0 when the given order is kept (perm is then the identity).  Host only. */
+int lddmm_spatial_order(const double *cen, int n, int *perm);
+
 /* FLOPs per pair interaction the roofline uses (FMA = 2, as executed), for the
  * shooting step, the fused adjoint step and the varifold pair of the given kinds. */
 double lddmm_flops_per_pair(int sweep, int dim, int knl_order, char cen_type, char dir_type);

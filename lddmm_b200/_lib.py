@@ -23,7 +23,7 @@ EXPORTS = [
     "lddmm_lbfgs", "lddmm_lbfgs_device", "lddmm_lbfgs_trace", "lddmm_shoot", "lddmm_LDDMM",
     "lddmm_elm_ifo", "lddmm_multiply_kernel", "lddmm_dq_kernel", "lddmm_varifold",
     "lddmm_flops_per_pair", "lddmm_ctx_time_sweeps", "lddmm_ctx_counters",
-    "lddmm_fp32_peak", "lddmm_pipe_peaks", "lddmm_multiply_kernel_noalloc", "lddmm_ctx_timeline",
+    "lddmm_fp32_peak", "lddmm_pipe_peaks", "lddmm_spatial_order", "lddmm_multiply_kernel_noalloc", "lddmm_ctx_timeline",
     "lddmm_ws_create", "lddmm_ws_destroy", "lddmm_ws_last_error", "lddmm_ws_num_params",
     "lddmm_ws_params", "lddmm_ws_grad", "lddmm_ws_train_step", "lddmm_ws_predict",
     "lddmm_ws_gemm_bf16", "lddmm_wait_selftest", "lddmm_compute_kernel",
@@ -116,6 +116,7 @@ def _load():
     L.lddmm_ctx_counters.argtypes = [C.c_void_p, C.POINTER(C.c_longlong), C.c_int]
     L.lddmm_fp32_peak.argtypes = [C.c_int, _dp]
     L.lddmm_pipe_peaks.argtypes = [C.c_int, _dp]
+    L.lddmm_spatial_order.argtypes = [_dp, C.c_int, C.POINTER(C.c_int)]
     L.lddmm_ctx_timeline.argtypes = [C.c_void_p, _dp]
     L.lddmm_wait_selftest.argtypes = [C.c_int, C.c_int, _dp]
     L.lddmm_multiply_kernel_noalloc.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p,

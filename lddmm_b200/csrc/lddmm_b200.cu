@@ -752,6 +752,16 @@ static std::vector<int> spatial_order(const std::vector<double> &cen, int n) {
   return {};
 }
 
+extern "C" int lddmm_spatial_order(const double *cen, int n, int *perm) {
+  if (!cen || n < 0 || !perm) {
+    set_err("lddmm_spatial_order: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  const std::vector<int> p = spatial_order(std::vector<double>(cen, cen + (size_t)n * 3), n);
+  for (int e = 0; e < n; ++e) perm[e] = p.empty() ? e : p[e];
+  return p.empty() ? 0 : 1;
+}
+
 static int device_sms(int dev) {
   int sms = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||

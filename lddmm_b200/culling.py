@@ -4,10 +4,11 @@ The varifold sweep (Gaussian centre kernel, k = 2^-|x|^2 in scaled centre
 coordinates x = c sqrt(log2 e) / cenKnlWidth) tests every (64-row tile, aligned
 32-column block) pair of a problem once: the block is skipped when the bounding box
 of its scaled centres lies farther than squared distance 64 from the box of the
-tile's 64 rows.  Which blocks survive depends only on the geometry, not on the
-launch shape, so the share of pair interactions that the sweep evaluates can be
-restated here exactly (up to the FP32 rounding of the boxes) for rooflines and
-tests.
+tile's 64 rows.  Which blocks survive depends only on the geometry and on the
+elements' storage order (which the library may change to a Morton order, see
+``spatial_order``), not on the launch shape, so the share of pair interactions that
+the sweep evaluates can be restated here exactly (up to the FP32 rounding of the
+boxes) for rooflines and tests.
 """
 from __future__ import annotations
 

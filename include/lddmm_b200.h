@@ -37,8 +37,10 @@
  * No entry point calls exit() or prints unless asked to (verbose).
  *
  * Threading: a context is used by one host thread at a time; distinct contexts are
- * independent.  The library keeps no mutable global state besides the per-thread
- * error message.
+ * independent.  Process-wide state, all of it guarded or per thread: the error
+ * message (per host thread), one stream-ordered device memory pool per device from
+ * which contexts take their memory (guarded by a mutex), and the fixed device array of
+ * lddmm_multiply_kernel_noalloc with its cached per-device address.
  */
 #ifndef LDDMM_B200_H
 #define LDDMM_B200_H
@@ -232,12 +234,16 @@ int lddmm_dq_kernel2(int dim, int ni, const double *qi, int nj, const double *qj
  * compiled into the library, which every GPU that loads the library holds until the
  * process exits.  Nothing is allocated.
  *
- * Limit: 1 <= n <= LDDMM_NOALLOC_MAX_POINTS; larger n returns LDDMM_ERR_ARG.
- * The first call on a device looks up the array's device address (with that device
- * current); make that first call before any stream capture.  Every call shares the
- * array: calls that overlap on the GPU (other streams, other host threads) race and
- * give wrong results; each call clears what must start at zero.  Asynchronous on
- * `stream` (a cudaStream_t, NULL for the default stream). */
+ * Limit: 1 <= n <= LDDMM_NOALLOC_MAX_POINTS; larger n returns LDDMM_ERR_ARG.  Every
+ * kernel order of lddmm_multiply_kernel is supported (2D and 3D: Gaussian -1, Matern
+ * 0..4).  The first call on a device looks up the array's device address (with that
+ * device current) and caches it for the life of the process; make that first call
+ * before any stream capture, and do not use this entry point after the device or its
+ * primary context has been reset (cudaDeviceReset, MATLAB's reset(gpuDevice)): the
+ * cached address would then be stale.  Every call shares the array: calls that
+ * overlap on the GPU (other streams, other host threads) race and give wrong results;
+ * each call clears what must start at zero.  Asynchronous on `stream` (a cudaStream_t,
+ * NULL for the default stream). */
 #define LDDMM_NOALLOC_MAX_POINTS 32768
 int lddmm_multiply_kernel_noalloc(int dim, int n, const double *d_q, const double *d_a,
                                   int knl_order, double knl_width, double *d_v, void *stream);

@@ -2392,8 +2392,24 @@ static cudaError_t noalloc_sweep(unsigned char *scratch, const double *q, const 
   op.vlc64 = v;
   op.tile_part = reinterpret_cast<double *>(scratch + kNaTile);
   op.t = 0;
-  return launch_sweep(op, reinterpret_cast<const int2 *>(scratch + kNaItems), ntiles,
-                      default_cluster(ntiles), stream);
+  // No programmatic stream serialisation here: the sweep reads its work list (written
+  // by noalloc_prepare_kernel just before) ahead of its dependency wait, which is only
+  // safe for the static lists of a context.  Without the attribute the sweep starts
+  // after the preparation kernel has completed.
+  const int S = default_cluster(ntiles);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(ntiles * S));
+  cfg.blockDim = dim3(kWarps * 32);
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)S;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, sweep_kernel<ShootOp<D, ORDER>, kWarps>, op,
+                            reinterpret_cast<const int2 *>(scratch + kNaItems), S);
 }
 
 extern "C" int lddmm_multiply_kernel_noalloc(int dim, int n, const double *d_q,
@@ -2412,7 +2428,7 @@ extern "C" int lddmm_multiply_kernel_noalloc(int dim, int n, const double *d_q,
     set_err("lddmm_multiply_kernel_noalloc: null buffer or non-positive width");
     return LDDMM_ERR_ARG;
   }
-  if (knl_order < -1 || knl_order > 4 || (dim == 2 && knl_order != -1)) {
+  if (knl_order < -1 || knl_order > 4) {
     set_err("lddmm_multiply_kernel_noalloc: kernel order %d in %dD not supported", knl_order,
             dim);
     return LDDMM_ERR_UNSUPPORTED;
@@ -2436,7 +2452,14 @@ extern "C" int lddmm_multiply_kernel_noalloc(int dim, int n, const double *d_q,
   CU(cudaGetLastError());
   cudaError_t e = cudaErrorInvalidValue;
   if (dim == 2) {
-    e = noalloc_sweep<2, -1>(scratch, d_q, d_a, d_v, ntiles, st);
+    switch (knl_order) {
+      case -1: e = noalloc_sweep<2, -1>(scratch, d_q, d_a, d_v, ntiles, st); break;
+      case 0: e = noalloc_sweep<2, 0>(scratch, d_q, d_a, d_v, ntiles, st); break;
+      case 1: e = noalloc_sweep<2, 1>(scratch, d_q, d_a, d_v, ntiles, st); break;
+      case 2: e = noalloc_sweep<2, 2>(scratch, d_q, d_a, d_v, ntiles, st); break;
+      case 3: e = noalloc_sweep<2, 3>(scratch, d_q, d_a, d_v, ntiles, st); break;
+      case 4: e = noalloc_sweep<2, 4>(scratch, d_q, d_a, d_v, ntiles, st); break;
+    }
   } else {
     switch (knl_order) {
       case -1: e = noalloc_sweep<3, -1>(scratch, d_q, d_a, d_v, ntiles, st); break;

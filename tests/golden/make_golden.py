@@ -26,7 +26,9 @@ sys.path.insert(0, ROOT)
 from lddmm_b200 import problem  # noqa: E402
 from oracle.oracle import Reference  # noqa: E402
 
-REF_TREE = os.environ.get("LDDMM_REFERENCE", "/root/reference")
+# the reference checkout: $LDDMM_REFERENCE, else `reference` beside the repository root
+REF_TREE = os.environ.get("LDDMM_REFERENCE",
+                          os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 def save(name, P=None, **arrays):

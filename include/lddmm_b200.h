@@ -94,7 +94,9 @@ typedef struct lddmm_opt {
 	double tol_val;           /* tolVal (OptimalityTolerance): stop when |g| < tol */
 	double wolfe1;            /* Armijo constant */
 	double wolfe2;            /* curvature constant */
-	int mem_num;              /* memNum (Columns), at most 32 */
+	int mem_num;              /* memNum (Columns), any size >= 1: the ring holds
+	                             min(memNum, itrMax) pairs (identical iterates);
+	                             LDDMM_ERR_NOMEM when that ring cannot fit the device */
 	int vbs_flg;              /* print the reference's iteration table per pair */
 	double rel_obj_tol;       /* additional stop: |f_prev - f| <= rel_obj_tol |f_prev|;
 	                             0 disables (the reference has only the |g| test) */

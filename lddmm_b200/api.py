@@ -332,7 +332,7 @@ def LDDMM(iniNdeMat, iniAlpStk, disObj, knlOrder, knlWidth, timeEnd, timeStp, op
                            tol=float(_scalar(o.get("OptimalityTolerance", 1e-6))),
                            wolfe1=float(_scalar(o.get("Wolfe1", 1e-4))),
                            wolfe2=float(_scalar(o.get("Wolfe2", 0.9))),
-                           mem_num=int(min(_scalar(o.get("Columns", min(100, nvar))), 32)),
+                           mem_num=int(_scalar(o.get("Columns", min(100, nvar)))),
                            verbose=bool(_scalar(o.get("Verbose", False))))
     alpStk = np.transpose(x.reshape(timeNum - 1, n, dim), (2, 1, 0))
     ndeStk, vlcStk = computeNodePosition(ini, alpStk, P.knl_order, P.knl_width, P.time_stp,

@@ -143,6 +143,7 @@ struct lddmm_ctx {
   int n_units = 0;            // (pair, row group) work units
   int n_segs = 0, n_slots = 0;
   int cycle_grid = 0;         // CTAs of the fused L-BFGS cycle kernel (0: per-pass launches)
+  int cycle_grid_lm = 0;      // the same for long L-BFGS memories (every co-resident CTA)
   int2 *units = nullptr;
   int4 *segs = nullptr;       // persistent work plan (persist.cuh)
   int *cta_seg = nullptr;
@@ -171,6 +172,7 @@ struct lddmm_ctx {
   double *X = nullptr, *G = nullptr, *XT = nullptr, *GT = nullptr, *Dv = nullptr;
   double *Sh = nullptr, *Yh = nullptr;
   double *SYm = nullptr, *YYm = nullptr, *coef = nullptr;  // compact-form L-BFGS state
+  double *RI = nullptr, *LV = nullptr, *SYd = nullptr, *LU = nullptr;  // long memory
   int m_alloc = 0;
   double *part = nullptr;
   double *rec = nullptr;
@@ -184,6 +186,7 @@ struct lddmm_ctx {
   OptParams loop_opt{};
   int *cyc = nullptr;  // cycles run by the device loop
   long long last_cycles = 0, last_launches = 0, last_evals = 0;
+  int last_mem = 0;  // L-BFGS memory (ring slots) of the last lddmm_lbfgs call
   int lbfgs_calls = 0;  // graphs are captured from the second L-BFGS call on
   bool use_graph = true;
   cudaGraphExec_t cycle_exec = nullptr;
@@ -224,6 +227,7 @@ lddmm_ctx::~lddmm_ctx() {
   dfree(XT, stream); dfree(GT, stream); dfree(Dv, stream);
   dfree(Sh, stream); dfree(Yh, stream); dfree(part, stream);
   dfree(SYm, stream); dfree(YYm, stream); dfree(coef, stream);
+  dfree(RI, stream); dfree(LV, stream); dfree(SYd, stream); dfree(LU, stream);
   dfree(rec, stream); dfree(sync, stream); dfree(units, stream); dfree(segs, stream);
   dfree(cta_seg, stream); dfree(unit_parts, stream); dfree(seg_part, stream);
   dfree(unit_cnt, stream);
@@ -1208,8 +1212,10 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
     int bc = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bc, lbfgs_cycle_kernel, kVecThreads, 0) ==
             cudaSuccess &&
-        bc > 0 && cf.persistent >= 0)
+        bc > 0 && cf.persistent >= 0) {
       c.cycle_grid = std::min(bc * sms, c.nchunk_tot);
+      c.cycle_grid_lm = bc * sms;
+    }
   }
   if (cf.autotune) {
     const int rc = autotune(c);
@@ -1390,24 +1396,42 @@ extern "C" int lddmm_shoot(lddmm_ctx *ctx, const double *alp, double *nde_stk, d
 
 // ==================================================================== L-BFGS
 
+// Device bytes of the memory-dependent L-BFGS buffers for memory m (s / y ring, Y^T Y,
+// coefficients, dot partials, and for m > kMaxMem the long-memory state).
+static size_t lbfgs_mem_bytes(const lddmm_ctx &c, long long m) {
+  const long long P = c.P, mc = std::max<long long>(m, kMaxMem);
+  long long d = 2 * m * c.nvar + P * m * m + P * (1 + 2 * mc) +
+                (long long)c.nchunk_tot * std::max<long long>(kPartStride, 4 * m);
+  if (m > kMaxMem) d += P * m * m + P * m * 7;
+  return (size_t)d * sizeof(double);
+}
+
 static cudaError_t ensure_lbfgs_buffers(lddmm_ctx &c, int m, int rec_cap) {
   if (!c.X) {
     CUE(dalloc(c.stream, &c.X, c.nvar));
     CUE(dalloc(c.stream, &c.G, c.nvar));
     CUE(dalloc(c.stream, &c.Dv, c.nvar));
-    CUE(dalloc(c.stream, &c.coef, (size_t)c.P * kCoefStride));
+    CUE(dalloc(c.stream, &c.SYm, (size_t)c.P * kMaxMem * kMaxMem));  // m <= kMaxMem only
   }
   if (c.m_alloc < m) {
-    dfree(c.Sh, c.stream);
-    dfree(c.Yh, c.stream);
-    dfree(c.SYm, c.stream);
-    dfree(c.YYm, c.stream);
-    CUE(dalloc(c.stream, &c.Sh, (size_t)m * c.nvar));
-    CUE(dalloc(c.stream, &c.Yh, (size_t)m * c.nvar));
-    CUE(dalloc(c.stream, &c.SYm, (size_t)c.P * m * m));
-    CUE(dalloc(c.stream, &c.YYm, (size_t)c.P * m * m));
+    dfree(c.Sh, c.stream); dfree(c.Yh, c.stream); dfree(c.YYm, c.stream);
+    dfree(c.coef, c.stream); dfree(c.part, c.stream);
+    dfree(c.RI, c.stream); dfree(c.LV, c.stream); dfree(c.SYd, c.stream); dfree(c.LU, c.stream);
+    const size_t mm = (size_t)m, mc = (size_t)std::max(m, kMaxMem);
+    CUE(dalloc(c.stream, &c.Sh, mm * c.nvar));
+    CUE(dalloc(c.stream, &c.Yh, mm * c.nvar));
+    CUE(dalloc(c.stream, &c.YYm, (size_t)c.P * mm * mm));
+    CUE(dalloc(c.stream, &c.coef, (size_t)c.P * (1 + 2 * mc)));
+    CUE(dalloc(c.stream, &c.part, (size_t)c.nchunk_tot * std::max<size_t>(kPartStride, 4 * mm)));
+    if (m > kMaxMem) {
+      CUE(dalloc(c.stream, &c.RI, (size_t)c.P * mm * mm));
+      CUE(dalloc(c.stream, &c.LV, (size_t)c.P * mm * 4));
+      CUE(dalloc(c.stream, &c.SYd, (size_t)c.P * mm));
+      CUE(dalloc(c.stream, &c.LU, (size_t)c.P * mm * 2));
+    }
     c.m_alloc = m;
     c.graph_valid = false;
+    c.loop_valid = false;
   }
   if (c.rec_cap < rec_cap) {
     dfree(c.rec, c.stream);
@@ -1436,12 +1460,17 @@ static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o,
   A.NPtot = c.NPtot;
   A.D = c.D;
   A.m = o.mem_num;
+  A.lm = o.mem_num > kMaxMem ? 1 : 0;
+  A.pstride = A.lm ? 4 * o.mem_num : kPartStride;
+  A.cstride = A.lm ? 1 + 2 * o.mem_num : kCoefStride;
+  A.RI = c.RI; A.LV = c.LV; A.SYd = c.SYd; A.LU = c.LU;
   const unsigned nb = (unsigned)c.nchunk_tot;
   const int pb = (c.P + 127) / 128;
   if (c.cycle_grid > 0) {
-    // the whole optimiser update in one cooperative launch
+    // the whole optimiser update in one cooperative launch (long memories: on every
+    // co-resident CTA, their phases have up to chunks x 8 units)
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)c.cycle_grid);
+    cfg.gridDim = dim3((unsigned)(A.lm ? c.cycle_grid_lm : c.cycle_grid));
     cfg.blockDim = dim3(kVecThreads);
     cfg.stream = c.stream;
     cudaLaunchAttribute attr[1];
@@ -1458,24 +1487,36 @@ static cudaError_t launch_cycle(lddmm_ctx &c, const OptParams &o,
   };
   CUE(pass(kPost));
   CUE(launch(decide_kernel, (unsigned)pb, 128, 0, c.stream, (const PairDesc *)c.pd, c.st, c.P,
-             (const double *)c.part, o, c.rec));
-  CUE(pass(kAccept));
-  CUE(launch(solve_kernel, (unsigned)c.P, kVecThreads, 0, c.stream, A));
-  CUE(pass(kFin));
+             (const double *)c.part, A.pstride, o, c.rec));
+  if (A.lm) {
+    const long long nslot = (long long)c.P * A.m;
+    const long long ngrp = (A.m + kLmGroup - 1) / kLmGroup;
+    const long long grid[7] = {c.nchunk_tot, c.nchunk_tot * ngrp, (nslot + 255) / 256,
+                               (nslot + 7) / 8, (nslot + 7) / 8, (nslot + 255) / 256,
+                               (long long)c.nchunk_tot * kLmSub};
+    for (int ph = kLmUpdate; ph <= kLmFin; ++ph)
+      CUE(launch(lm_phase_kernel, (unsigned)grid[ph], kVecThreads, 0, c.stream, A, ph, c.P,
+                 c.nchunk_tot));
+  } else {
+    CUE(pass(kAccept));
+    CUE(launch(solve_kernel, (unsigned)c.P, kVecThreads, 0, c.stream, A));
+    CUE(pass(kFin));
+  }
   CUE(launch(ls_init_kernel, (unsigned)pb, 128, 0, c.stream, (const PairDesc *)c.pd, c.st, c.P,
-             (const double *)c.part, c.act));
+             (const double *)c.part, A.pstride, A.lm ? kLmSub : 1, c.act));
   if (max_cycles > 0)
     CUE(launch(cycle_control_kernel, 1, 256, 0, c.stream, h, (const int *)c.act, c.P, c.cyc,
                max_cycles, (const StepSync *)c.sync));
   return cudaSuccess;
 }
 
-static long long kernels_per_cycle(const lddmm_ctx &c) {
+static long long kernels_per_cycle(const lddmm_ctx &c, int m) {
   // objective: T shooting + [geometry + varifold] + gather + objective + T adjoint
   // (2 launches when the time loops are persistent); optimiser: POST, DECIDE, ACCEPT,
-  // SOLVE, FIN, LSINIT (1 launch when fused)
+  // SOLVE, FIN, LSINIT, or POST, DECIDE, the 7 long-memory phases, LSINIT (1 launch
+  // when fused)
   const long long sweeps = c.persistent ? 2 : 2LL * c.T;
-  const long long opt = c.cycle_grid > 0 ? 1 : 6;
+  const long long opt = c.cycle_grid > 0 ? 1 : (m > kMaxMem ? 10 : 6);
   return sweeps + 2 + (c.has_vfd ? 2 : 0) + opt;
 }
 
@@ -1571,14 +1612,29 @@ static void print_table(const lddmm_ctx &c, int p, const std::vector<double> &re
 
 static int lbfgs_run(lddmm_ctx &c, const lddmm_opt *opt, const double *alp, bool host,
                      double *alp_out, lddmm_result *res) {
-  if (!opt || opt->mem_num < 1 || opt->mem_num > kMaxMem || opt->itr_max < 0 || !(opt->tol_val >= 0)) {
-    set_err("lddmm_lbfgs: bad options (mem_num must be 1..%d)", kMaxMem);
+  if (!opt || opt->mem_num < 1 || opt->itr_max < 0 || !(opt->tol_val >= 0)) {
+    set_err("lddmm_lbfgs: bad options (mem_num >= 1, itr_max >= 0, tol_val >= 0)");
     return LDDMM_ERR_ARG;
   }
   OptParams o;
   std::memset(&o, 0, sizeof(o));
   o.itr_max = opt->itr_max;
-  o.mem_num = opt->mem_num;
+  // The ring never holds more pairs than there are accepted iterations, and a ring
+  // that never wraps behaves the same whatever its size (LBFGS.cpp:96-99: slot newIdx
+  // advances once per iteration, getDirection uses min(itr - 1, memNum) pairs), so
+  // min(memNum, itrMax) slots give the reference's iterates exactly for any memNum.
+  o.mem_num = std::min(opt->mem_num, std::max(opt->itr_max, 1));
+  if (o.mem_num > c.m_alloc) {
+    size_t fr = 0, tot = 0;
+    CU(cudaSetDevice(c.device));
+    CU(cudaMemGetInfo(&fr, &tot));
+    const size_t need = lbfgs_mem_bytes(c, o.mem_num);
+    if (need > fr + lbfgs_mem_bytes(c, c.m_alloc)) {
+      set_err("lddmm_lbfgs: an L-BFGS memory of %d pairs needs %.2f GB of device memory, "
+              "%.2f GB are free", o.mem_num, need / 1e9, fr / 1e9);
+      return LDDMM_ERR_NOMEM;
+    }
+  }
   o.tol = opt->tol_val;
   o.wolfe1 = opt->wolfe1;
   o.wolfe2 = opt->wolfe2;
@@ -1653,7 +1709,8 @@ static int lbfgs_run(lddmm_ctx &c, const lddmm_opt *opt, const double *alp, bool
     }
   }
   c.last_cycles = cycles;
-  c.last_launches = cycles * kernels_per_cycle(c) + 2;
+  c.last_launches = cycles * kernels_per_cycle(c, o.mem_num) + 2;
+  c.last_mem = o.mem_num;
   CU(cudaMemcpyAsync(hs.data(), c.st, sizeof(PairState) * c.P, cudaMemcpyDeviceToHost, c.stream));
   CU(cudaMemcpyAsync(alp_out, c.X, sizeof(double) * c.nvar,
                      host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, c.stream));
@@ -1756,7 +1813,7 @@ extern "C" int lddmm_ctx_counters(const lddmm_ctx *ctx, long long *out, int n) {
                           ctx->last_launches, ctx->last_evals};
   const int k = std::min(n, 4);
   for (int i = 0; i < k; ++i) out[i] = v[i];
-  if (k >= 2 && ctx->last_cycles) out[1] = kernels_per_cycle(*ctx);
+  if (k >= 2 && ctx->last_cycles) out[1] = kernels_per_cycle(*ctx, ctx->last_mem);
   return k;
 }
 

@@ -83,18 +83,36 @@ def two_set_kernels(dim, seed):
     save(f"two_set_kernels_{dim}d", **arrays)
 
 
-def sphere2cube_example():
+def _sphere2cube_example_problem():
     import scipy.io as sio
     ex = os.path.join(REF_TREE, "Cpp", "examples", "sphere2cube")
     s = sio.loadmat(os.path.join(ex, "sphereData.mat"))
     c = sio.loadmat(os.path.join(ex, "cubeData.mat"))
     sel = np.arange(0, c["tgtCenPosMat"].shape[1], 10)
     # parameters of Cpp/examples/sphere2cube/run_sphere2cube.m:14-24
-    P = problem.Problem(s["iniNdeMat"].T, s["elmVtxMat"].T.astype(np.int32) - 1,
-                        c["tgtCenPosMat"].T[sel], c["tgtUniDirMat"].T[sel],
-                        c["tgtElmVolVec"].ravel()[sel], knl_order=3, knl_width=0.25,
-                        time_num=21, time_stp=0.05, cen_type="C", cen_width=0.1,
-                        dir_type="B", dir_width=0.0, dis_wgt=100.0)
+    return problem.Problem(s["iniNdeMat"].T, s["elmVtxMat"].T.astype(np.int32) - 1,
+                           c["tgtCenPosMat"].T[sel], c["tgtUniDirMat"].T[sel],
+                           c["tgtElmVolVec"].ravel()[sel], knl_order=3, knl_width=0.25,
+                           time_num=21, time_stp=0.05, cen_type="C", cen_width=0.1,
+                           dir_type="B", dir_width=0.0, dis_wgt=100.0)
+
+
+def sphere2cube_example_columns():
+    """The reference's example optimiser options as run_sphere2cube.m:27-31 passes them
+    (Columns = 10000, Wolfe 0 / 0.5, tolerance 1e-2), for 40 iterations: the history
+    grows past 32 pairs.  The reference allocates the whole ring of 10000 (s, y) pairs
+    (Cpp/src/LDDMM.cpp:58-60; 5.8 GB here)."""
+    P = _sphere2cube_example_problem()
+    R = Reference(3)
+    r = R.lbfgs(P, np.zeros(P.var_num), itr_max=40, tol=1e-2, wolfe1=0.0, wolfe2=0.5,
+                mem_num=10000)
+    save("sphere2cube_example_columns", x=r["x"], f=np.array(r["f"]), ret=np.array(r["ret"]),
+         trace_f=r["trace_f"], trace_g2=r["trace_g2"],
+         opt=np.array([40, 1e-2, 0.0, 0.5, 10000]))
+
+
+def sphere2cube_example():
+    P = _sphere2cube_example_problem()
     R = Reference(3)
     rng = np.random.default_rng(11)
     alp = rng.normal(size=P.var_num) * 0.02
@@ -196,14 +214,21 @@ def objgrd_orders_2d():
     save("objgrd_orders_2d", P, alp=alp, **arrays)
 
 
+ALL = {
+    "kernels_2d": lambda: kernels(2, 1),
+    "kernels_3d": lambda: kernels(3, 2),
+    "two_set_kernels_2d": lambda: two_set_kernels(2, 11),
+    "two_set_kernels_3d": lambda: two_set_kernels(3, 12),
+    "circle2square": circle2square,
+    "circle2square_example": circle2square_example,
+    "sphere2cube_example": sphere2cube_example,
+    "sphere2cube_example_columns": sphere2cube_example_columns,
+    "varifold_types": varifold_types,
+    "objgrd_orders_3d": objgrd_orders_3d,
+    "objgrd_orders_2d": objgrd_orders_2d,
+}
+
 if __name__ == "__main__":
-    kernels(2, 1)
-    kernels(3, 2)
-    two_set_kernels(2, 11)
-    two_set_kernels(3, 12)
-    circle2square()
-    circle2square_example()
-    sphere2cube_example()
-    varifold_types()
-    objgrd_orders_3d()
-    objgrd_orders_2d()
+    # python tests/golden/make_golden.py [name ...]   (no names: every fixture)
+    for name in (sys.argv[1:] or list(ALL)):
+        ALL[name]()

@@ -1,0 +1,63 @@
+"""Whole registrations at the workloads' own sizes against the compiled reference's
+own FP64 registrations (tests/golden/make_converged.py): the final objective within
+1e-5 relative and the final landmarks within 1e-4 of the shape diameter (RMS over
+landmarks), the two correctness criteria of the hot path.
+
+The FP32 path and the FP64 reference start from the same zero momenta, take the same
+first iterations (the early traces are pinned in test_gpu_lbfgs.py) and then drift
+apart at the FP32 rounding level; what is compared here is where both end up after
+the same iteration budget.  Final landmarks: the trajectory of the returned momenta
+(computeNodePosition, Cpp/src/computeNodePosition.m:1-20, here lddmm_shoot).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _register(P, itr_max):
+    from lddmm_b200 import api
+
+    with api.Context(P) as ctx:
+        x, res = ctx.lbfgs(np.zeros(P.var_num), itr_max=itr_max, tol=1e-6, wolfe1=1e-4,
+                           wolfe2=0.9, mem_num=5)
+        (nde, _), = ctx.shoot(x)
+    return res[0], nde[-1]
+
+
+def _check(P, z, r, nde):
+    f_ref = float(z["f"])
+    rel_f = abs(r["f"] - f_ref) / abs(f_ref)
+    err = np.sqrt(np.mean(np.sum((nde - z["nde_final"]) ** 2, axis=1))) / P.diameter()
+    print(f"f {r['f']:.9g} vs reference {f_ref:.9g} (rel {rel_f:.2e}); landmarks RMS "
+          f"{err:.2e} of the diameter; iterations {r['iters']}, status {r['status']}")
+    assert r["status"] in (0, 3), r  # 3: bracketed at the FP32 noise floor near the end
+    assert rel_f < 1e-5, rel_f
+    assert err < 1e-4, err
+
+
+def test_circle2square_300_iterations_against_the_reference():
+    """2D circle -> square, 200 landmarks, 300 iterations (the reference: 320
+    evaluations)."""
+    from lddmm_b200 import problem
+
+    z = golden("circle2square_300")
+    P = problem.circle_to_square()
+    r, nde = _register(P, int(z["itr_max"]))
+    _check(P, z, r, nde)
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(GOLDEN, "sphere2cube_500.npz")),
+                    reason="fixture not generated")
+def test_sphere2cube_500_iterations_against_the_reference():
+    """3D sphere -> cube, 2562 landmarks, 500 iterations."""
+    from lddmm_b200 import problem
+
+    z = golden("sphere2cube_500")
+    P = problem.sphere_to_cube()
+    r, nde = _register(P, int(z["itr_max"]))
+    _check(P, z, r, nde)

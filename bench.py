@@ -9,8 +9,10 @@ one whole registration.  Synthetic data, generated deterministically.
 
 Metric: registrations/s (whole job, all ranks); the JSON line also reports pair
 interactions/s, the objective's relative error against the FP64 oracle at the
-returned point, the FP32 roofline of the dominant sweep, and the reference's C++
-path timed on the host cores.
+returned point, the FP32 roofline of the dominant sweep, the reference's C++ path
+timed on the host cores, and (key "population") the uneven 256-pair batch registered
+in one context to 1e-5 relative objective change next to the reference's FP64 GPU
+path on a seeded stratified sample of its pairs, measured in the same run.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -38,6 +40,15 @@ WORKLOAD = "sphere2cube: icosphere 2562 v / 5120 t -> cube 12288 t, Matern nu=3/
            "varifold G(0.15) x Binet, T=20, L-BFGS m=5, <=500 iterations"
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
 BATCH_PAIRS = 8  # registrations in the batched-form measurement
+# the config object both arms print (identical, so that the two lines compare)
+CONFIG = {"workload": WORKLOAD,
+          "l2": "GPU arm: 256 MiB device memset before every timed registration; "
+                "CPU arm: not applicable"}
+POP_PAIRS = 256  # the uneven population: pairs registered together in one context
+POP_SAMPLE = 32  # population pairs also registered by the reference's FP64 GPU path
+POP_WORKLOAD = ("population: 256 star-shaped pairs (seed 0), 500-20000 landmarks and "
+                "1000-40000 target triangles log-uniform, Gaussian 0.3, varifold G(0.1) x "
+                "Binet, T=10, to 1e-5 relative objective change")
 
 # The FP64 registration of this workload (CPU oracle, 500 iterations; generator
 # tests/golden/make_c2_reference.py): its objective is what a registration has to
@@ -57,6 +68,8 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--itr", type=int, default=500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-population", action="store_true",
+                    help="skip the 256-pair population leg and its FP64 GPU baseline")
     ap.add_argument("--mode", choices=["registration", "objgrd", "large_pair", "ws_gemm"],
                     default="registration",
                     help="objgrd: only time device-resident objective+gradient evaluations "
@@ -198,7 +211,7 @@ def run_reference(args):
         "ms_per_step": wall / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": WORKLOAD, "sample": "objgrd evaluations"},
+        "config": CONFIG,
         "cpu_baseline": {
             "value": value, "unit": UNIT, "cores": n, "kind": kind,
             "sample": f"{n} processes x one objective+gradient evaluation per step "
@@ -208,6 +221,105 @@ def run_reference(args):
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------- population (uneven batch)
+
+def population_leg(stream, local, flush):
+    """The uneven 256-pair population registered in one context (one launch per sweep
+    for all pairs, the L-BFGS loop as one device-side graph), to 1e-5 relative
+    objective change, device-resident, CUDA events on the context stream; next to it
+    the reference's plain FP64 GPU path (CUDA/src compiled unmodified, oracle/_ref) on
+    a seeded stratified sample of the same pairs, each run for the iterations that
+    pair took here, and this build's batch of exactly that sample."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from lddmm_b200 import _lib, api, problem
+    from oracle.oracle import ReferenceCuda
+
+    t0 = time.perf_counter()
+    probs = problem.population(POP_PAIRS, seed=0, workers=max(1, min(os.cpu_count() or 1, 32)))
+    t_gen = time.perf_counter() - t0
+
+    def batch(ps, reps):
+        with api.Context(ps, stream=stream.cuda_stream, device=local) as ctx:
+            d = torch.zeros(ctx.var_total, dtype=torch.float64, device="cuda")
+            res = (_lib.Result * len(ps))()
+
+            def run(itr):
+                o = _lib.Opt(itr, 1e-12, 1e-4, 0.9, 5, 0, 1e-5)
+                d.zero_()
+                rc = _lib.lib.lddmm_lbfgs_device(ctx.handle, C.byref(o),
+                                                 C.c_void_p(d.data_ptr()), res)
+                if rc < 0 and rc != -3:
+                    _lib.check(rc)
+
+            run(2)  # the context's first L-BFGS call (host-driven cycles)
+            ms = []
+            for _ in range(reps):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                run(2000)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            return statistics.median(ms), [dict(iters=r.iters, evals=r.evals, status=r.status,
+                                                f=r.fcn) for r in res], ctx.counters()
+
+    with ClockSampler(local) as clk:
+        ms_all, res_all, cnt = batch(probs, 2)
+    clocks = clk.summary()
+    pairs_eval = [2 * P.T * P.nde_num ** 2 + P.dfm_elm_num * (P.dfm_elm_num + P.tgt_elm_num)
+                  for P in probs]
+    inter = sum(r["evals"] * w + P.tgt_elm_num ** 2
+                for r, w, P in zip(res_all, pairs_eval, probs))
+
+    # stratified sample: pairs sorted by their work here, POP_SAMPLE strata of equal
+    # count, one pair drawn per stratum (seeded); the FP64 time of the whole population
+    # is estimated as the sum over strata of (stratum size x the drawn pair's time)
+    work = np.array([r["evals"] * w for r, w in zip(res_all, pairs_eval)], dtype=np.float64)
+    order = np.argsort(work, kind="stable")
+    strata = np.array_split(order, POP_SAMPLE)
+    rng = np.random.default_rng(1)
+    pick = [int(st[rng.integers(0, len(st))]) for st in strata]
+    R = ReferenceCuda(3)
+    p0 = probs[pick[0]]
+    R.lbfgs(p0, np.zeros(p0.var_num), itr_max=1, tol=1e-12)  # library start-up
+    ref = []
+    for k in pick:
+        P = probs[k]
+        r = R.lbfgs(P, np.zeros(P.var_num), itr_max=max(1, res_all[k]["iters"]), tol=1e-12)
+        ref.append(dict(pair=k, landmarks=P.nde_num, iters=res_all[k]["iters"],
+                        evals=r["evals"], ms_lbfgs=r["ms_lbfgs"], ms_total=r["ms_total"]))
+    ref_lbfgs_s = sum(r["ms_lbfgs"] for r in ref) * 1e-3
+    ref_total_s = sum(r["ms_total"] for r in ref) * 1e-3
+    est_lbfgs_s = sum(len(st) * r["ms_lbfgs"] for st, r in zip(strata, ref)) * 1e-3
+    ms_sample, _, _ = batch([probs[k] for k in pick], 2)
+    secs = ms_all * 1e-3
+    return {
+        "workload": POP_WORKLOAD, "pairs": POP_PAIRS,
+        "registrations_per_s": POP_PAIRS / secs, "seconds": secs,
+        "gpair_interactions_per_s": inter / secs / 1e9,
+        "iters_median": float(np.median([r["iters"] for r in res_all])),
+        "iters_max": int(max(r["iters"] for r in res_all)),
+        "status": sorted({int(r["status"]) for r in res_all}),
+        "kernel_launches": cnt["launches"], "generation_s": t_gen, "clocks": clocks,
+        "fp64_gpu_reference": {
+            "path": "reference CUDA/src (FP64, cuBLAS), compiled unmodified for sm_100a",
+            "sample": f"{POP_SAMPLE} pairs, one per stratum of the pairs sorted by work "
+                      f"(seed 1); each run for the iterations it took here",
+            "sample_seconds_lbfgs": ref_lbfgs_s, "sample_seconds_total": ref_total_s,
+            "population_seconds_estimated": est_lbfgs_s,
+            "pairs": ref},
+        "ours_sample_seconds": ms_sample * 1e-3,
+        "speedup_vs_fp64_gpu_same_sample": ref_lbfgs_s / (ms_sample * 1e-3),
+        "speedup_vs_fp64_gpu_population_estimated": est_lbfgs_s / secs,
+    }
 
 
 # ----------------------------------------------------------------- our arm
@@ -292,14 +404,12 @@ def run_ours(args):
     torch.cuda.synchronize()
     replicas.barrier(dist)
     e_steps = max(1, min(args.steps, 3))
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
+    # lddmm_LDDMM is synchronous (it returns with optAlpVec in host memory): host wall
+    # time around the calls is the end-to-end time
+    t0 = time.perf_counter()
     for _ in range(e_steps):
         _lib.check(min(e2e_call(), 0))
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e_ms = replicas.max_over_ranks(dist, e0.elapsed_time(e1), "cuda")
+    e_ms = replicas.max_over_ranks(dist, (time.perf_counter() - t0) * 1e3, "cuda")
     h2d = (ini.nbytes + alp0.nbytes + P.elm_vtx.nbytes + ifo.nbytes + P.tgt_cen.nbytes
            + P.tgt_dir.nbytes + P.tgt_vol.nbytes)
     d2h = out.nbytes
@@ -331,6 +441,10 @@ def run_ours(args):
             batched = {"pairs": BATCH_PAIRS, "registrations_per_s": BATCH_PAIRS / (b_ms * 1e-3),
                        "ms_per_batch": b_ms,
                        "iters": [r.iters for r in res_b], "status": [r.status for r in res_b]}
+
+    population = None
+    if rank == 0 and world == 1 and not args.no_population:
+        population = population_leg(stream, local, flush)
 
     # roofline of the dominant sweep: live per-launch timing (CUDA events on the
     # context stream) of one evaluation at the returned point
@@ -391,8 +505,8 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 kernels + f64 optimiser", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "parallelism": f"replicas x{world}",
-                       "l2": "256 MiB memset before every registration",
+            "config": CONFIG,
+            "details": {"parallelism": f"replicas x{world}",
                        "iters": iters, "status": status, "evals_per_registration": evals_per_reg,
                        "f_final": f_final, "rel_err_f_vs_fp64_oracle": rel_f,
                        "f_fp64_registration": FP64_REGISTRATION["f"],
@@ -414,6 +528,7 @@ def run_ours(args):
             "gpu_launches": launches,
             "clocks": clocks,
             "batched": batched,
+            "population": population,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -92,24 +92,27 @@ def elm_ifo(elm_vtx: np.ndarray, nde_num: int) -> np.ndarray:
     E, V = ev.shape
     if V not in (2, 3):
         raise ValueError("elements must have 2 or 3 vertices")
-    cnt = np.bincount(ev.ravel(), minlength=nde_num)
+    flat = ev.ravel()
+    cnt = np.bincount(flat, minlength=nde_num)
     rows = 1 + int(cnt.max() if cnt.size else 0) * V
     out = np.zeros((nde_num, rows), dtype=np.int32)
-    fill = np.zeros(nde_num, dtype=np.int64)
-    other = {0: (2, 1), 1: (0, 2), 2: (1, 0)}
-    for e in range(E):
-        for k in range(V):
-            v = ev[e, k]
-            a = fill[v]
-            fill[v] += 1
-            if V == 2:
-                out[v, 1 + 2 * a] = e
-                out[v, 2 + 2 * a] = -1 if k == 0 else 1
-            else:
-                out[v, 1 + 3 * a] = e
-                out[v, 2 + 3 * a] = ev[e, other[k][0]]
-                out[v, 3 + 3 * a] = ev[e, other[k][1]]
-    out[:, 0] = fill
+    # entry (e, k) of vertex v = ev[e, k]; a vertex's entries in increasing element order
+    # (a stable sort of the element-major list by vertex), a = rank within the vertex
+    order = np.argsort(flat, kind="stable")
+    v_sorted = flat[order]
+    start = np.concatenate([[0], np.cumsum(cnt)[:-1]])
+    a = np.arange(flat.size) - start[v_sorted]
+    e, k = order // V, order % V
+    if V == 2:
+        out[v_sorted, 1 + 2 * a] = e
+        out[v_sorted, 2 + 2 * a] = np.where(k == 0, -1, 1)
+    else:
+        o1 = np.array([2, 0, 1])[k]  # the other two vertices: (2, 1), (0, 2), (1, 0)
+        o2 = np.array([1, 2, 0])[k]
+        out[v_sorted, 1 + 3 * a] = e
+        out[v_sorted, 2 + 3 * a] = ev[e, o1]
+        out[v_sorted, 3 + 3 * a] = ev[e, o2]
+    out[:, 0] = cnt
     return out
 
 
@@ -173,25 +176,37 @@ def star_pair(src_subdiv: int = 7, tgt_subdiv: int = 6, lmax: int = 8, sigma: fl
                    dis_wgt=dis_wgt, name="star_pair")
 
 
+def _population_pair(args) -> Problem:
+    k, nv, nt, ps, lmax, sigma, sigma_v, sigma_w, time_num = args
+    V, F = shapes.decimated_star(nv, lmax, sigma, ps)
+    # a closed triangulation of the sphere with nt triangles has nt/2 + 2 vertices
+    tv, tf = shapes.decimated_star(max(nt // 2 + 2, 12), lmax, sigma, ps + 1)
+    cen, dr, vol = shapes.varifold_of(tv, tf)
+    T = time_num - 1
+    return Problem(V, F, cen, dr, vol, knl_order=-1, knl_width=sigma_v, time_num=time_num,
+                   time_stp=1.0 / T, cen_type="G", cen_width=sigma_w, dir_type="B",
+                   dis_wgt=1.0, name=f"pop{k}")
+
+
 def population(n_pairs: int = 256, seed: int = 0, n_min: int = 500, n_max: int = 20000,
                t_min: int = 1000, t_max: int = 40000, lmax: int = 8, sigma: float = 0.05,
-               sigma_v: float = 0.3, sigma_w: float = 0.1, time_num: int = 11):
+               sigma_v: float = 0.3, sigma_w: float = 0.1, time_num: int = 11,
+               workers: int = 1):
     """Batch of independent star-shaped pairs with log-uniform vertex counts in
     [n_min, n_max] (random vertex decimation) and log-uniform target triangle counts
-    in [t_min, t_max]."""
+    in [t_min, t_max].  workers > 1 builds the meshes in that many spawned processes
+    (same pairs: every random draw of the sizes and seeds happens here, in order)."""
     rng = np.random.default_rng(seed)
-    probs = []
+    jobs = []
     for k in range(n_pairs):
         nv = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
         nt = int(round(math.exp(rng.uniform(math.log(t_min), math.log(t_max)))))
         ps = int(rng.integers(0, 2**31 - 1))
-        V, F = shapes.decimated_star(nv, lmax, sigma, ps)
-        # a closed triangulation of the sphere with nt triangles has nt/2 + 2 vertices
-        tv, tf = shapes.decimated_star(max(nt // 2 + 2, 12), lmax, sigma, ps + 1)
-        cen, dr, vol = shapes.varifold_of(tv, tf)
-        T = time_num - 1
-        probs.append(Problem(V, F, cen, dr, vol, knl_order=-1, knl_width=sigma_v,
-                             time_num=time_num, time_stp=1.0 / T, cen_type="G",
-                             cen_width=sigma_w, dir_type="B", dis_wgt=1.0,
-                             name=f"pop{k}"))
-    return probs
+        jobs.append((k, nv, nt, ps, lmax, sigma, sigma_v, sigma_w, time_num))
+    if workers <= 1:
+        return [_population_pair(j) for j in jobs]
+    import concurrent.futures as cf
+    import multiprocessing as mp
+
+    with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_population_pair, jobs, chunksize=4))

@@ -101,3 +101,44 @@ def test_star_surface_and_population_sizes():
         assert 100 <= P.nde_num <= 400
         assert P.T == 10
         assert np.all(P.tgt_vol > 0)
+
+
+def test_elm_ifo_matches_the_element_loop():
+    """The vectorised getElmIfo table equals a direct loop over the elements
+    (Cpp/src/getElmIfo.m:1-59 semantics) on a 3D mesh and a 2D polyline."""
+    from lddmm_b200 import problem, shapes
+
+    def loop(ev, n):
+        E, V = ev.shape
+        cnt = np.bincount(ev.ravel(), minlength=n)
+        out = np.zeros((n, 1 + int(cnt.max()) * V), dtype=np.int32)
+        fill = np.zeros(n, dtype=np.int64)
+        other = {0: (2, 1), 1: (0, 2), 2: (1, 0)}
+        for e in range(E):
+            for k in range(V):
+                v = ev[e, k]
+                a = fill[v]
+                fill[v] += 1
+                if V == 2:
+                    out[v, 1 + 2 * a], out[v, 2 + 2 * a] = e, (-1 if k == 0 else 1)
+                else:
+                    out[v, 1 + 3 * a] = e
+                    out[v, 2 + 3 * a] = ev[e, other[k][0]]
+                    out[v, 3 + 3 * a] = ev[e, other[k][1]]
+        out[:, 0] = fill
+        return out
+
+    V, F = shapes.decimated_star(700, 6, 0.05, 3)
+    assert np.array_equal(problem.elm_ifo(F, V.shape[0]), loop(F, V.shape[0]))
+    cv, ce = shapes.circle(50)
+    assert np.array_equal(problem.elm_ifo(ce, 50), loop(ce, 50))
+
+
+def test_population_workers_build_the_same_pairs():
+    from lddmm_b200 import problem
+
+    a = problem.population(n_pairs=3, seed=4, n_max=2000, t_max=3000)
+    b = problem.population(n_pairs=3, seed=4, n_max=2000, t_max=3000, workers=2)
+    for x, y in zip(a, b):
+        assert np.array_equal(x.ini_nde, y.ini_nde) and np.array_equal(x.elm_vtx, y.elm_vtx)
+        assert np.array_equal(x.tgt_cen, y.tgt_cen) and np.array_equal(x.elm_ifo, y.elm_ifo)

@@ -107,7 +107,12 @@ typedef struct lddmm_config {
 	int cluster_shoot;        /* CTAs per i-tile (thread-block cluster size, 1..8) */
 	int cluster_adjoint;
 	int cluster_varifold;
-	int autotune;             /* 1: time the candidate cluster sizes at creation */
+	int autotune;             /* 0 (default) or 1: time the candidate launch shapes at
+	                             creation (per-step sweeps: 1 or 2 64-row tiles per work
+	                             item x cluster split 1/2/4/8; varifold split 1..8;
+	                             persistent time loops vs per-step launches) and keep
+	                             the fastest, cached per batch shape for the process;
+	                             -1: the built-in rule, no timing */
 	int use_graph;            /* 1 (default): capture the L-BFGS cycle in a CUDA graph */
 	void *stream;             /* cudaStream_t to run on; NULL: the context creates one */
 	int device;               /* CUDA device ordinal (default 0) */
@@ -145,6 +150,10 @@ long long lddmm_ctx_var_total(const lddmm_ctx *ctx);
 void *lddmm_ctx_stream(const lddmm_ctx *ctx);
 /* Cluster sizes in use (after autotuning): out[0..2] = shoot, adjoint, varifold. */
 int lddmm_ctx_launch_config(const lddmm_ctx *ctx, int *out3);
+/* Launch shape in use: out[0..2] cluster sizes (shoot, adjoint, varifold), out[3..4]
+ * 64-row tiles per work item of the shooting / adjoint sweeps, out[5] 1 when the time
+ * loops run as persistent launches.  Returns 6. */
+int lddmm_ctx_launch_shape(const lddmm_ctx *ctx, int *out6);
 
 /* Objective and gradient of every pair at alp (concatenated, host memory);
  * fcn[num], grd like alp.  objgrd.cpp:26 semantics. */

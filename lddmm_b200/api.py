@@ -38,7 +38,7 @@ def _problem_struct(P: Problem, keep: list) -> _lib.Problem:
 class Context:
     """A batch of pairs on the GPU (``lddmm_ctx``)."""
 
-    def __init__(self, problems, cluster=(0, 0, 0), autotune=False, use_graph=True,
+    def __init__(self, problems, cluster=(0, 0, 0), autotune=None, use_graph=True,
                  stream=None, device=0, persistent=0):
         if isinstance(problems, Problem):
             problems = [problems]
@@ -46,7 +46,10 @@ class Context:
         keep: list = []
         arr = (_lib.Problem * len(self.problems))(
             *[_problem_struct(P, keep) for P in self.problems])
-        cfg = _lib.Config(cluster[0], cluster[1], cluster[2], 1 if autotune else 0,
+        # autotune: None -> the library default (on), True -> on, False -> off (the
+        # built-in launch-shape rule)
+        tune = 0 if autotune is None else (1 if autotune else -1)
+        cfg = _lib.Config(cluster[0], cluster[1], cluster[2], tune,
                           1 if use_graph else -1, stream, device, persistent)
         h = C.c_void_p()
         check(lib.lddmm_ctx_create(arr, len(self.problems), C.byref(cfg), C.byref(h)))
@@ -82,6 +85,14 @@ class Context:
         o = np.zeros(3, dtype=np.int32)
         check(lib.lddmm_ctx_launch_config(self._h, iptr(o)))
         return tuple(int(x) for x in o)
+
+    def launch_shape(self):
+        """dict(cluster=(shoot, adjoint, varifold), tiles=(shoot, adjoint),
+        persistent=bool): the launch shape the context runs (after autotuning)."""
+        o = np.zeros(6, dtype=np.int32)
+        check(lib.lddmm_ctx_launch_shape(self._h, iptr(o)))
+        return dict(cluster=tuple(int(x) for x in o[:3]), tiles=(int(o[3]), int(o[4])),
+                    persistent=bool(o[5]))
 
     def time_sweeps(self, reps=3):
         """Average ms per launch: shooting step, adjoint step, varifold sweep, and

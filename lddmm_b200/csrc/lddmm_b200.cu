@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <memory>
+#include <map>
 #include <mutex>
 #include <utility>
 #include <cstdarg>
@@ -137,6 +138,7 @@ struct lddmm_ctx {
   int n_pt_items = 0, n_el_items = 0;
   int n_pt_items2 = 0;  // two-tile items of the per-step shooting sweep
   int S_shoot = 1, S_adj = 1, S_vfd = 1;
+  int tpw_shoot = 1, tpw_adj = 1;  // 64-row tiles per work item of the per-step sweeps
   // persistent multi-step sweeps (one cooperative launch per direction)
   bool persistent = false;
   int pers_ctas = 0;          // CTAs of the persistent kernels (one share of work each)
@@ -286,12 +288,13 @@ static cudaError_t shoot_impl(lddmm_ctx &c, int t, double *vlc) {
   op.vlc64 = vlc;
   op.tile_part = c.reg_part + (size_t)t * c.ntile_tot;
   op.t = t;
-  // packed FP32x2 form of the same sweep (bitwise the same sums).  The Gaussian kernel
-  // runs on two-tile items, each staged column serving four rows per lane: its sweep
-  // is held first by the shared-memory reads (163,842 landmarks: 11.13 -> 10.58 ms);
-  // the Matern kernels, with a square root per pair and fewer CTAs per SM at the
-  // larger register count, are faster on single tiles (40,962: 1.02 vs 1.10 ms).
-  if constexpr (ORDER == -1)
+  // packed FP32x2 form of the same sweep (bitwise the same sums), on one- or two-tile
+  // work items (c.tpw_shoot; the default rule and the autotuner pick it).  Two tiles
+  // per item serve four rows per lane from each staged column: the Gaussian sweep,
+  // held first by the shared-memory reads, gains (163,842 landmarks: 11.13 -> 10.58
+  // ms); the Matern kernels, with a square root per pair and fewer CTAs per SM at the
+  // larger register count, were faster on single tiles (40,962: 1.02 vs 1.10 ms).
+  if (c.tpw_shoot == 2)
     return launch(sweep_packed_kernel<ShootOp<D, ORDER>, kWarps, 2>,
                   (unsigned)(c.n_pt_items2 * c.S_shoot), kWarps * 32, c.S_shoot, c.stream, op,
                   (const int2 *)c.pt_items2, c.S_shoot);
@@ -317,10 +320,10 @@ static cudaError_t adjoint_impl(lddmm_ctx &c, int t, double *g, double *pdot) {
   op.ls_n = (t > 0) ? c.ls + (size_t)((t - 1) & 1) * c.NPtot : nullptr;
   op.pdot64 = pdot;
   op.t = t;
-  // packed FP32x2 form of the same sweep (bitwise the same sums); the Gaussian kernel
-  // on two-tile items as in shoot_impl (163,842 landmarks: 23.3 -> 22.0 ms at 2 CTAs
-  // per SM instead of 3)
-  if constexpr (ORDER == -1)
+  // packed FP32x2 form of the same sweep (bitwise the same sums), one- or two-tile
+  // items as in shoot_impl (c.tpw_adj; Gaussian at 163,842 landmarks: 23.3 -> 22.0 ms
+  // with two tiles, at 2 CTAs per SM instead of 3)
+  if (c.tpw_adj == 2)
     return launch(sweep_packed_kernel<AdjointOp<D, ORDER>, kWarps, 2>,
                   (unsigned)(c.n_pt_items2 * c.S_adj), kWarps * 32, c.S_adj, c.stream, op,
                   (const int2 *)c.pt_items2, c.S_adj);
@@ -777,7 +780,7 @@ static int device_sms(int dev) {
 static cudaError_t run_eval(lddmm_ctx &c, double *g_out, double *f_out, double *vlc,
                             bool grad);
 
-static int autotune(lddmm_ctx &c);
+static int autotune(lddmm_ctx &c, const lddmm_config &cf);
 
 extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm_config *cfg,
                                 lddmm_ctx **out) {
@@ -1174,6 +1177,8 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
       if (c.n_el_items <= c.vfd_clusters(s)) S = s;
     if (S) c.S_vfd = S;
   }
+  // two-tile work items for the Gaussian per-step sweeps, one tile for the Matern ones
+  c.tpw_shoot = c.tpw_adj = (c.order == -1) ? 2 : 1;
   for (int *s : {&c.S_shoot, &c.S_adj, &c.S_vfd})
     if (*s < 1 || *s > 8) {
       set_err("cluster sizes must be 1..8");
@@ -1217,8 +1222,8 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
       c.cycle_grid_lm = bc * sms;
     }
   }
-  if (cf.autotune) {
-    const int rc = autotune(c);
+  if (cf.autotune >= 0) {
+    const int rc = autotune(c, cf);
     if (rc) return rc;
   }
   *out = cp.release();
@@ -1271,6 +1276,17 @@ extern "C" int lddmm_ctx_launch_config(const lddmm_ctx *c, int *o) {
   o[1] = c->S_adj;
   o[2] = c->S_vfd;
   return 0;
+}
+
+extern "C" int lddmm_ctx_launch_shape(const lddmm_ctx *c, int *o) {
+  if (!c || !o) return LDDMM_ERR_ARG;
+  o[0] = c->S_shoot;
+  o[1] = c->S_adj;
+  o[2] = c->S_vfd;
+  o[3] = c->tpw_shoot;
+  o[4] = c->tpw_adj;
+  o[5] = c->persistent ? 1 : 0;
+  return 6;
 }
 
 // ================================================================ objective
@@ -1906,46 +1922,144 @@ extern "C" int lddmm_ctx_time_sweeps(lddmm_ctx *ctx, int reps, double *ms4) {
 
 // =============================================================== autotuner
 
-static int autotune(lddmm_ctx &c) {
-  // Time every cluster size for each sweep on this batch (zero momenta; the cost
-  // does not depend on the values) and keep the fastest.
+// Choices of the autotuner, cached per launch signature for the life of the process
+// (a later context of the same shapes starts with them, without timing anything).
+struct TuneChoice {
+  int S_shoot, S_adj, S_vfd, tpw_shoot, tpw_adj, persistent;
+};
+static std::mutex g_tune_mu;
+static std::map<std::string, TuneChoice> g_tune_cache;
+
+static std::string tune_key(const lddmm_ctx &c, const lddmm_config &cf) {
+  std::string k;
+  auto add = [&](long long v) { k += std::to_string(v) + ","; };
+  add(c.device); add(c.D); add(c.order); add(c.ct); add(c.dt); add(c.T); add(c.has_vfd);
+  add(c.persistent); add(cf.cluster_shoot); add(cf.cluster_adjoint); add(cf.cluster_varifold);
+  add(cf.persistent);
+  for (const PairDesc &d : c.hpd) {
+    add(d.Npad); add(d.Edpad); add(d.Etpad);
+  }
+  return k;
+}
+
+// Median milliseconds of `reps` timed runs of f (after one untimed run).
+template <class F>
+static cudaError_t time_median(lddmm_ctx &c, cudaEvent_t e0, cudaEvent_t e1, int reps, F &&f,
+                               float *ms_out) {
+  std::vector<float> ms;
+  for (int r = 0; r <= reps; ++r) {
+    CUE(cudaEventRecord(e0, c.stream));
+    CUE(f());
+    CUE(cudaEventRecord(e1, c.stream));
+    CUE(cudaEventSynchronize(e1));
+    float t = 0.0f;
+    CUE(cudaEventElapsedTime(&t, e0, e1));
+    if (r > 0) ms.push_back(t);
+  }
+  std::sort(ms.begin(), ms.end());
+  *ms_out = ms[ms.size() / 2];
+  return cudaSuccess;
+}
+
+static int autotune(lddmm_ctx &c, const lddmm_config &cf) {
+  // The launch shape of each sweep, chosen by timing the candidates on this batch
+  // (zero momenta; the cost does not depend on the values): per-step shooting and
+  // adjoint sweeps over one or two 64-row tiles per work item and a cluster split S of
+  // 1, 2, 4 or 8 CTAs per item; the varifold sweep over S = 1..8; and, for a batch on
+  // the persistent time-loop sweeps, those against T per-step launches of the tuned
+  // shape.  Sizes given in the configuration are kept.  Every candidate gives the same
+  // sums up to the order in which a cluster's partial sums are added (two-tile items
+  // are bitwise one-tile items), so the choice affects time only.
+  const std::string key = tune_key(c, cf);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      const TuneChoice &t = it->second;
+      c.S_shoot = t.S_shoot; c.S_adj = t.S_adj; c.S_vfd = t.S_vfd;
+      c.tpw_shoot = t.tpw_shoot; c.tpw_adj = t.tpw_adj; c.persistent = t.persistent != 0;
+      return 0;
+    }
+  }
   CU(launch_set_active(c, c.P));
+  if (c.has_vfd) CU(launch_geometry(c, c.q64));  // element boxes of the initial surface
   cudaEvent_t e0, e1;
   CU(cudaEventCreate(&e0));
   CU(cudaEventCreate(&e1));
-  const int cands[4] = {1, 2, 4, 8};
-  int *slots[3] = {&c.S_shoot, &c.S_adj, &c.S_vfd};
-  for (int which = 0; which < 3; ++which) {
-    if (which == 2 && !c.has_vfd) break;
+  const int reps = 3;
+  cudaError_t err = cudaSuccess;
+  auto tune_step = [&](int which, int *S, int *tpw, bool fixS) {
     float best = 1e30f;
-    int bestS = *slots[which];
-    for (int S : cands) {
-      *slots[which] = S;
-      float ms = 0.0f;
-      for (int rep = 0; rep < 4; ++rep) {
-        CU(cudaEventRecord(e0, c.stream));
-        cudaError_t e = (which == 0) ? c.shoot(c, 0, nullptr)
-                        : (which == 1) ? c.adjoint(c, 0, c.GT, nullptr)
-                                       : c.varifold(c);
-        CU(e);
-        CU(cudaEventRecord(e1, c.stream));
-        CU(cudaEventSynchronize(e1));
-        float t = 0.0f;
-        CU(cudaEventElapsedTime(&t, e0, e1));
-        if (rep > 0) ms += t;
+    int bS = *S, bT = *tpw;
+    for (int T2 = 1; T2 <= 2 && err == cudaSuccess; ++T2)
+      for (int Sc : {1, 2, 4, 8}) {
+        if (fixS && Sc != bS) continue;
+        *S = Sc;
+        *tpw = T2;
+        float ms = 0.0f;
+        err = time_median(c, e0, e1, reps, [&]() {
+          return which == 0 ? c.shoot(c, 0, nullptr) : c.adjoint(c, 0, c.GT, nullptr);
+        }, &ms);
+        if (err != cudaSuccess) break;
+        if (ms < best) {
+          best = ms;
+          bS = Sc;
+          bT = T2;
+        }
       }
-      if (ms < best) {
+    *S = bS;
+    *tpw = bT;
+  };
+  tune_step(0, &c.S_shoot, &c.tpw_shoot, cf.cluster_shoot > 0);
+  tune_step(1, &c.S_adj, &c.tpw_adj, cf.cluster_adjoint > 0);
+  if (err == cudaSuccess && c.has_vfd && cf.cluster_varifold <= 0) {
+    float best = 1e30f;
+    int bS = c.S_vfd;
+    for (int Sc = 1; Sc <= 8 && err == cudaSuccess; ++Sc) {
+      c.S_vfd = Sc;
+      float ms = 0.0f;
+      err = time_median(c, e0, e1, reps, [&]() { return c.varifold(c); }, &ms);
+      if (err == cudaSuccess && ms < best) {
         best = ms;
-        bestS = S;
+        bS = Sc;
       }
     }
-    *slots[which] = bestS;
+    c.S_vfd = bS;
+  }
+  if (err == cudaSuccess && c.persistent && cf.persistent == 0) {
+    // whole time loops: one persistent launch per direction against T launches
+    float mp = 0.0f, ms = 0.0f;
+    err = reset_sync(c);
+    if (err == cudaSuccess)
+      err = time_median(c, e0, e1, reps, [&]() {
+        cudaError_t e = c.shoot_all(c, nullptr);
+        return e == cudaSuccess ? c.adjoint_all(c, c.GT) : e;
+      }, &mp);
+    if (err == cudaSuccess) {
+      const int rc = check_sync(c);  // the persistent trials' bounded waits
+      if (rc) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return rc;
+      }
+      err = time_median(c, e0, e1, reps, [&]() {
+        cudaError_t e = cudaSuccess;
+        for (int t = 0; t < c.T && e == cudaSuccess; ++t) e = c.shoot(c, t, nullptr);
+        for (int t = c.T - 1; t >= 0 && e == cudaSuccess; --t) e = c.adjoint(c, t, c.GT, nullptr);
+        return e;
+      }, &ms);
+    }
+    if (err == cudaSuccess && ms < mp) c.persistent = false;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  CU(err);
   // the trial sweeps wrote the step-1 positions and adjoint state; reset them
   CU(cudaMemsetAsync(c.p64, 0, sizeof(double) * c.NPtot * c.D, c.stream));
   CU(cudaStreamSynchronize(c.stream));
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = TuneChoice{c.S_shoot, c.S_adj, c.S_vfd, c.tpw_shoot, c.tpw_adj,
+                                 c.persistent ? 1 : 0};
   return 0;
 }
 

@@ -117,8 +117,11 @@ typedef struct lddmm_config {
 	void *stream;             /* cudaStream_t to run on; NULL: the context creates one */
 	int device;               /* CUDA device ordinal (default 0) */
 	int persistent;           /* time loops as one persistent cooperative launch per
-	                             direction: 1 on, -1 off, 0 automatic (on when one step
-	                             of the batch does not fill the GPU) */
+	                             direction: 0 automatic (when one step of the batch does
+	                             not fill the GPU; the form chosen by the autotuner),
+	                             1 on (split row groups combined through L2), 2 on
+	                             (thread-block clusters own whole row groups and combine
+	                             them through distributed shared memory), -1 off */
 } lddmm_config;
 
 /* Per-pair outcome of lddmm_lbfgs. */
@@ -151,8 +154,9 @@ void *lddmm_ctx_stream(const lddmm_ctx *ctx);
 /* Cluster sizes in use (after autotuning): out[0..2] = shoot, adjoint, varifold. */
 int lddmm_ctx_launch_config(const lddmm_ctx *ctx, int *out3);
 /* Launch shape in use: out[0..2] cluster sizes (shoot, adjoint, varifold), out[3..4]
- * 64-row tiles per work item of the shooting / adjoint sweeps, out[5] 1 when the time
- * loops run as persistent launches.  Returns 6. */
+ * 64-row tiles per work item of the shooting / adjoint sweeps, out[5] the form of
+ * the time loops (0 per-step launches, 1 persistent with L2 combine, 2 persistent
+ * cluster form).  Returns 6. */
 int lddmm_ctx_launch_shape(const lddmm_ctx *ctx, int *out6);
 
 /* Objective and gradient of every pair at alp (concatenated, host memory);

@@ -88,11 +88,13 @@ class Context:
 
     def launch_shape(self):
         """dict(cluster=(shoot, adjoint, varifold), tiles=(shoot, adjoint),
-        persistent=bool): the launch shape the context runs (after autotuning)."""
+        persistent=0 | 1 | 2): the launch shape the context runs (after autotuning);
+        persistent 0: per-step launches, 1: persistent time loops combining split row
+        groups in L2, 2: the cluster form."""
         o = np.zeros(6, dtype=np.int32)
         check(lib.lddmm_ctx_launch_shape(self._h, iptr(o)))
         return dict(cluster=tuple(int(x) for x in o[:3]), tiles=(int(o[3]), int(o[4])),
-                    persistent=bool(o[5]))
+                    persistent=int(o[5]))
 
     def time_sweeps(self, reps=3):
         """Average ms per launch: shooting step, adjoint step, varifold sweep, and

@@ -20,9 +20,13 @@
 #include "lbfgs.cuh"
 #include "ops.cuh"
 #include "persist.cuh"
+#include "plan.h"
 #include "sweep.cuh"
 
 using namespace lddmm;
+
+static_assert(lddmm::kPlanSub == lddmm::kSub, "plan sub-tile");
+static_assert(lddmm::kPlanMaxJobParts == lddmm::kMaxJobParts, "plan job parts");
 
 namespace {
 
@@ -142,6 +146,13 @@ struct lddmm_ctx {
   // persistent multi-step sweeps (one cooperative launch per direction)
   bool persistent = false;
   int pers_ctas = 0;          // CTAs of the persistent kernels (one share of work each)
+  // cluster form of the persistent sweeps (persist.cuh persistent_cluster_kernel):
+  // pers_kind 1 runs it, on pers_cl_ctas CTAs in clusters of pers_C; 0 the L2 form
+  int pers_kind = 0, pers_C = 0, pers_cl_ctas = 0;
+  long long pers_cl_share = 0, pers_l2_share = 0;  // largest CTA share of each plan
+  int4 *cl_segs = nullptr;
+  int *cl_cta_seg = nullptr, *cl_job_src = nullptr;
+  int2 *cl_job = nullptr;
   int n_units = 0;            // (pair, row group) work units
   int n_segs = 0, n_slots = 0;
   int cycle_grid = 0;         // CTAs of the fused L-BFGS cycle kernel (0: per-pass launches)
@@ -201,6 +212,9 @@ struct lddmm_ctx {
   cudaError_t (*shoot_all)(lddmm_ctx &, double *vlc) = nullptr;
   cudaError_t (*adjoint_all)(lddmm_ctx &, double *g) = nullptr;
   int (*pers_blocks)(int which) = nullptr;  // resident CTAs per SM of the persistent kernels
+  // co-resident clusters of C CTAs of the cluster-form persistent kernels (min of both)
+  int (*pers_clusters)(int C, int grid) = nullptr;
+  cudaError_t (*probe_cluster)(lddmm_ctx &) = nullptr;  // a cluster-form launch, no steps
   cudaError_t (*varifold)(lddmm_ctx &) = nullptr;
   int (*vfd_clusters)(int S) = nullptr;  // co-resident clusters of S varifold CTAs
   cudaError_t (*tt)(lddmm_ctx &, int p, double *part, dim3 grid, double cw, double dw) = nullptr;
@@ -233,6 +247,8 @@ lddmm_ctx::~lddmm_ctx() {
   dfree(rec, stream); dfree(sync, stream); dfree(units, stream); dfree(segs, stream);
   dfree(cta_seg, stream); dfree(unit_parts, stream); dfree(seg_part, stream);
   dfree(unit_cnt, stream);
+  dfree(cl_segs, stream); dfree(cl_cta_seg, stream); dfree(cl_job, stream);
+  dfree(cl_job_src, stream);
   dfree(dbb, stream); dfree(tbb, stream);
   if (own_stream && stream) cudaStreamDestroy(stream);
 }
@@ -336,7 +352,30 @@ static cudaError_t adjoint_impl(lddmm_ctx &c, int t, double *g, double *pdot) {
 // Cooperative launch of a persistent multi-step sweep (all CTAs co-resident; the
 // runtime refuses the launch otherwise).
 template <class Op>
-static cudaError_t launch_persistent(lddmm_ctx &c, const Op &op, int dir) {
+static cudaError_t launch_persistent(lddmm_ctx &c, const Op &op, int dir, int T = -1) {
+  if (T < 0) T = c.T;
+  if (c.pers_kind == 1) {
+    ClusterSweepPlan cp;
+    cp.units = c.units;
+    cp.segs = c.cl_segs;
+    cp.cta_seg = c.cl_cta_seg;
+    cp.job = c.cl_job;
+    cp.job_src = c.cl_job_src;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)c.pers_cl_ctas);
+    cfg.blockDim = dim3(kPersistWarps * 32);
+    cfg.stream = c.stream;
+    cudaLaunchAttribute attr[2];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    attr[1].id = cudaLaunchAttributeClusterDimension;
+    attr[1].val.clusterDim.x = (unsigned)c.pers_C;
+    attr[1].val.clusterDim.y = 1;
+    attr[1].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 2;
+    return cudaLaunchKernelEx(&cfg, persistent_cluster_kernel<Op>, op, cp, T, dir, c.sync);
+  }
   SweepPlan plan;
   plan.units = c.units;
   plan.segs = c.segs;
@@ -353,7 +392,7 @@ static cudaError_t launch_persistent(lddmm_ctx &c, const Op &op, int dir) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, persistent_sweep_kernel<Op>, op, plan, c.T, dir, c.sync);
+  return cudaLaunchKernelEx(&cfg, persistent_sweep_kernel<Op>, op, plan, T, dir, c.sync);
 }
 
 template <int D, int ORDER>
@@ -387,6 +426,52 @@ static cudaError_t adjoint_all_impl(lddmm_ctx &c, double *g) {
   op.ls0 = c.ls;
   op.NP = c.NPtot;
   return launch_persistent(c, op, -1);
+}
+
+// Co-resident clusters of C CTAs of both cluster-form persistent kernels.
+template <int D, int ORDER>
+static int pers_clusters_impl(int C, int grid) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(grid / C * C));
+  cfg.blockDim = dim3(kPersistWarps * 32);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int a = 0, b = 0;
+  if (cudaOccupancyMaxActiveClusters(&a, persistent_cluster_kernel<ShootOp<D, ORDER>>, &cfg) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveClusters(&b, persistent_cluster_kernel<AdjointOp<D, ORDER>>, &cfg) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return std::min(a, b);
+}
+
+// One launch of the cluster-form kernel with no steps: whether the runtime accepts a
+// cooperative launch of clusters of this size and grid.
+template <int D, int ORDER>
+static cudaError_t probe_cluster_impl(lddmm_ctx &c) {
+  ShootOp<D, ORDER> op;
+  op.pd = c.pd;
+  op.act = c.act;
+  op.x64 = c.XT;
+  op.qs0 = c.qs;
+  op.as0 = c.as;
+  op.q640 = c.q64;
+  op.vlc0 = nullptr;
+  op.reg0 = c.reg_part;
+  op.NP = c.NPtot;
+  op.ntile = c.ngrp_tot;
+  const int kind = c.pers_kind;
+  c.pers_kind = 1;
+  const cudaError_t e = launch_persistent(c, op, +1, 0);
+  c.pers_kind = kind;
+  return e;
 }
 
 template <int D, int ORDER>
@@ -437,6 +522,8 @@ static void set_def(lddmm_ctx &c) {
   c.shoot_all = shoot_all_impl<D, ORDER>;
   c.adjoint_all = adjoint_all_impl<D, ORDER>;
   c.pers_blocks = pers_blocks_impl<D, ORDER>;
+  c.pers_clusters = pers_clusters_impl<D, ORDER>;
+  c.probe_cluster = probe_cluster_impl<D, ORDER>;
 }
 
 template <int D>
@@ -626,70 +713,6 @@ extern "C" int lddmm_elm_ifo(const int *elm_vtx, int vpe, int elm_num, int nde_n
       }
     }
   return rows;
-}
-
-// Work plan of the persistent sweeps: the step's work (row groups x their j ranges,
-// laid end to end in unit order) cut into G contiguous shares, one per CTA.  Cuts
-// inside a row group are rounded to the 32-entry sub-tile and moved to the row group's
-// edge when they would leave a part shorter than kMinPart entries.  With little work
-// per CTA (under kSplitMin entries) row groups are not cut at all: each CTA takes whole
-// row groups and G is at most the row-group count.
-struct HostPlan {
-  std::vector<int4> segs;       // (unit, j begin, j end, part) in CTA order
-  std::vector<int> cta_seg;     // G + 1 offsets into segs
-  std::vector<int2> unit_parts; // (parts, first partial slot)
-  int slots = 0;
-};
-
-constexpr long long kMinPart = 32;
-constexpr long long kSplitMin = 512;
-
-static HostPlan plan_sweeps(const std::vector<int2> &units, const std::vector<PairDesc> &hpd,
-                            int G_max) {
-  const int nu = (int)units.size();
-  std::vector<long long> us(nu + 1, 0);
-  for (int u = 0; u < nu; ++u) us[u + 1] = us[u] + hpd[units[u].x].Npad;
-  const long long W = us[nu];
-  const bool cut = W / std::max(G_max, 1) >= kSplitMin;
-  const int G = cut ? G_max : std::max(1, std::min(G_max, nu));
-  std::vector<long long> b(G + 1, 0);
-  b[G] = W;
-  for (int k = 1; k < G; ++k) {
-    long long x;
-    if (cut) {
-      const long long w = W * k / G;
-      int u = (int)(std::upper_bound(us.begin(), us.end(), w) - us.begin()) - 1;
-      u = std::min(std::max(u, 0), nu - 1);
-      const long long J = us[u + 1] - us[u];
-      long long off = (w - us[u] + kSub / 2) / kSub * kSub;
-      if (off < kMinPart) off = 0;
-      else if (J - off < kMinPart) off = J;
-      x = us[u] + off;
-    } else {
-      x = us[(long long)nu * k / G];
-    }
-    b[k] = std::max(b[k - 1], std::min(x, W));
-  }
-  HostPlan h;
-  h.cta_seg.assign(G + 1, 0);
-  h.unit_parts.assign(nu, make_int2(0, 0));
-  std::vector<int> parts(nu, 0);
-  int u0 = 0;
-  for (int k = 0; k < G; ++k) {
-    h.cta_seg[k] = (int)h.segs.size();
-    while (u0 < nu && us[u0 + 1] <= b[k]) ++u0;
-    for (int v = u0; v < nu && us[v] < b[k + 1]; ++v) {
-      const long long lo = std::max(b[k], us[v]) - us[v];
-      const long long hi = std::min(b[k + 1], us[v + 1]) - us[v];
-      if (hi > lo) h.segs.push_back(make_int4(v, (int)lo, (int)hi, parts[v]++));
-    }
-  }
-  h.cta_seg[G] = (int)h.segs.size();
-  for (int v = 0; v < nu; ++v) {
-    h.unit_parts[v] = make_int2(parts[v], h.slots);
-    if (parts[v] > 1) h.slots += parts[v];
-  }
-  return h;
 }
 
 static int default_cluster(int n_items, int sms = 148) {
@@ -1197,6 +1220,7 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
     c.persistent = cap > 0 && (cf.persistent > 0 ||
                                (cf.persistent == 0 && c.n_units <= kPersistAutoUnits * cap));
     CU(dalloc(c.stream, &c.sync, 1));
+    CU(cudaMemsetAsync(c.sync, 0, sizeof(StepSync), c.stream));
     if (c.persistent) {
       const HostPlan h = plan_sweeps(uni, c.hpd, cap);
       c.pers_ctas = (int)h.cta_seg.size() - 1;
@@ -1213,6 +1237,62 @@ extern "C" int lddmm_ctx_create(const lddmm_problem *probs, int num, const lddmm
                          cudaMemcpyHostToDevice, c.stream));
       CU(cudaMemcpyAsync(c.unit_parts, h.unit_parts.data(), sizeof(int2) * h.unit_parts.size(),
                          cudaMemcpyHostToDevice, c.stream));
+      // the cluster form: the cluster size whose plan has the smallest CTA share
+      long long l2_share = 0;
+      for (int k = 0; k < c.pers_ctas; ++k) {
+        long long sh = 0;
+        for (int q = h.cta_seg[k]; q < h.cta_seg[k + 1]; ++q) sh += h.segs[q].z - h.segs[q].y;
+        l2_share = std::max(l2_share, sh);
+      }
+      ClusterHostPlan best;
+      int bestC = 0, best_ncl = 0;
+      for (int C = 1; C <= kMaxJobParts; ++C) {
+        const int ncl = std::min(c.pers_clusters(C, cap), cap / C);
+        if (ncl < 1) continue;
+        ClusterHostPlan ch = plan_cluster_sweeps(uni, c.hpd, C, ncl);
+        if (ch.ok && (!bestC || ch.max_share < best.max_share)) {
+          best = std::move(ch);
+          bestC = C;
+          best_ncl = ncl;
+        }
+      }
+      if (bestC) {
+        c.pers_C = bestC;
+        c.pers_cl_ctas = best_ncl * bestC;
+        CU(dalloc(c.stream, &c.cl_segs, std::max<size_t>(best.segs.size(), 1)));
+        CU(dalloc(c.stream, &c.cl_cta_seg, best.cta_seg.size()));
+        CU(dalloc(c.stream, &c.cl_job, best.job.size()));
+        CU(dalloc(c.stream, &c.cl_job_src, best.job_src.size()));
+        CU(cudaMemcpyAsync(c.cl_segs, best.segs.data(), sizeof(int4) * best.segs.size(),
+                           cudaMemcpyHostToDevice, c.stream));
+        CU(cudaMemcpyAsync(c.cl_cta_seg, best.cta_seg.data(), sizeof(int) * best.cta_seg.size(),
+                           cudaMemcpyHostToDevice, c.stream));
+        CU(cudaMemcpyAsync(c.cl_job, best.job.data(), sizeof(int2) * best.job.size(),
+                           cudaMemcpyHostToDevice, c.stream));
+        CU(cudaMemcpyAsync(c.cl_job_src, best.job_src.data(), sizeof(int) * best.job_src.size(),
+                           cudaMemcpyHostToDevice, c.stream));
+        c.pers_cl_share = best.max_share;
+        c.pers_l2_share = l2_share;
+        // default: the cluster form unless its balance is clearly worse than the L2
+        // form's (it saves the L2 round trips of the split row groups every step)
+        c.pers_kind = cf.persistent == 2  ? 1
+                      : cf.persistent == 1 ? 0
+                                           : ((best.max_share * 100 <= l2_share * 115) ? 1 : 0);
+        // the runtime must accept a cooperative launch of these clusters
+        cudaError_t pe = c.probe_cluster(c);
+        if (pe == cudaSuccess) pe = cudaStreamSynchronize(c.stream);
+        if (pe != cudaSuccess) {
+          cudaGetLastError();  // a refused launch configuration is not sticky
+          c.pers_kind = 0;
+          c.pers_C = 0;
+        }
+        CU(cudaMemsetAsync(c.sync, 0, sizeof(StepSync), c.stream));
+      }
+      if (cf.persistent == 2 && c.pers_C == 0) {
+        set_err("the cluster form of the persistent sweeps is not available for this batch "
+                "on this device");
+        return LDDMM_ERR_UNSUPPORTED;
+      }
     }
     int bc = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bc, lbfgs_cycle_kernel, kVecThreads, 0) ==
@@ -1285,7 +1365,7 @@ extern "C" int lddmm_ctx_launch_shape(const lddmm_ctx *c, int *o) {
   o[2] = c->S_vfd;
   o[3] = c->tpw_shoot;
   o[4] = c->tpw_adj;
-  o[5] = c->persistent ? 1 : 0;
+  o[5] = c->persistent ? 1 + c->pers_kind : 0;
   return 6;
 }
 
@@ -1925,7 +2005,7 @@ extern "C" int lddmm_ctx_time_sweeps(lddmm_ctx *ctx, int reps, double *ms4) {
 // Choices of the autotuner, cached per launch signature for the life of the process
 // (a later context of the same shapes starts with them, without timing anything).
 struct TuneChoice {
-  int S_shoot, S_adj, S_vfd, tpw_shoot, tpw_adj, persistent;
+  int S_shoot, S_adj, S_vfd, tpw_shoot, tpw_adj, persistent, pers_kind;
 };
 static std::mutex g_tune_mu;
 static std::map<std::string, TuneChoice> g_tune_cache;
@@ -1978,6 +2058,7 @@ static int autotune(lddmm_ctx &c, const lddmm_config &cf) {
       const TuneChoice &t = it->second;
       c.S_shoot = t.S_shoot; c.S_adj = t.S_adj; c.S_vfd = t.S_vfd;
       c.tpw_shoot = t.tpw_shoot; c.tpw_adj = t.tpw_adj; c.persistent = t.persistent != 0;
+      c.pers_kind = t.pers_kind;
       return 0;
     }
   }
@@ -2026,15 +2107,23 @@ static int autotune(lddmm_ctx &c, const lddmm_config &cf) {
     }
     c.S_vfd = bS;
   }
-  if (err == cudaSuccess && c.persistent && cf.persistent == 0) {
-    // whole time loops: one persistent launch per direction against T launches
-    float mp = 0.0f, ms = 0.0f;
-    err = reset_sync(c);
-    if (err == cudaSuccess)
-      err = time_median(c, e0, e1, reps, [&]() {
+  if (err == cudaSuccess && c.persistent) {
+    // whole time loops: the persistent forms (L2 combine; cluster combine when the
+    // runtime accepted it) against T per-step launches of the tuned shape
+    auto time_loops = [&](float *ms) {
+      return time_median(c, e0, e1, reps, [&]() {
         cudaError_t e = c.shoot_all(c, nullptr);
         return e == cudaSuccess ? c.adjoint_all(c, c.GT) : e;
-      }, &mp);
+      }, ms);
+    };
+    err = reset_sync(c);
+    float mk[2] = {1e30f, 1e30f};
+    const int k0 = cf.persistent == 2 ? 1 : 0;
+    const int k1 = (cf.persistent == 1 || !c.pers_C) ? 0 : 1;
+    for (int kind = k0; kind <= k1 && err == cudaSuccess; ++kind) {
+      c.pers_kind = kind;
+      err = time_loops(&mk[kind]);
+    }
     if (err == cudaSuccess) {
       const int rc = check_sync(c);  // the persistent trials' bounded waits
       if (rc) {
@@ -2042,14 +2131,18 @@ static int autotune(lddmm_ctx &c, const lddmm_config &cf) {
         cudaEventDestroy(e1);
         return rc;
       }
+    }
+    c.pers_kind = (mk[1] < mk[0]) ? 1 : 0;
+    if (err == cudaSuccess && cf.persistent == 0) {
+      float ms = 0.0f;
       err = time_median(c, e0, e1, reps, [&]() {
         cudaError_t e = cudaSuccess;
         for (int t = 0; t < c.T && e == cudaSuccess; ++t) e = c.shoot(c, t, nullptr);
         for (int t = c.T - 1; t >= 0 && e == cudaSuccess; --t) e = c.adjoint(c, t, c.GT, nullptr);
         return e;
       }, &ms);
+      if (err == cudaSuccess && ms < std::min(mk[0], mk[1])) c.persistent = false;
     }
-    if (err == cudaSuccess && ms < mp) c.persistent = false;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -2059,7 +2152,7 @@ static int autotune(lddmm_ctx &c, const lddmm_config &cf) {
   CU(cudaStreamSynchronize(c.stream));
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune_cache[key] = TuneChoice{c.S_shoot, c.S_adj, c.S_vfd, c.tpw_shoot, c.tpw_adj,
-                                 c.persistent ? 1 : 0};
+                                 c.persistent ? 1 : 0, c.pers_kind};
   return 0;
 }
 

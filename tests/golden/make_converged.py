@@ -2,6 +2,7 @@
 
     make -C oracle ref
     python tests/golden/make_converged.py circle2square_300    # seconds
+    python tests/golden/make_converged.py circle2square_converged  # minutes
     python tests/golden/make_converged.py sphere2cube_500      # ~1 h, one core
 
 circle2square_300: the 2D circle -> square workload (200 landmarks on the unit
@@ -51,6 +52,9 @@ def _run(name, P, itr_max):
 
 ALL = {
     "circle2square_300": lambda: _run("circle2square_300", problem.circle_to_square(), 300),
+    # the same registration run until |g| < 1e-6 (or 20000 iterations)
+    "circle2square_converged": lambda: _run("circle2square_converged",
+                                            problem.circle_to_square(), 20000),
     "sphere2cube_500": lambda: _run("sphere2cube_500", problem.sphere_to_cube(), 500),
 }
 

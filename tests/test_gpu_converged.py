@@ -29,7 +29,7 @@ def _register(P, itr_max):
     return res[0], nde[-1]
 
 
-def _check(P, z, r, nde):
+def _check(P, z, r, nde, lm_tol=1e-4):
     f_ref = float(z["f"])
     rel_f = abs(r["f"] - f_ref) / abs(f_ref)
     err = np.sqrt(np.mean(np.sum((nde - z["nde_final"]) ** 2, axis=1))) / P.diameter()
@@ -37,15 +37,31 @@ def _check(P, z, r, nde):
           f"{err:.2e} of the diameter; iterations {r['iters']}, status {r['status']}")
     assert r["status"] in (0, 3), r  # 3: bracketed at the FP32 noise floor near the end
     assert rel_f < 1e-5, rel_f
-    assert err < 1e-4, err
+    assert err < lm_tol, err
 
 
 def test_circle2square_300_iterations_against_the_reference():
-    """2D circle -> square, 200 landmarks, 300 iterations (the reference: 320
-    evaluations)."""
+    """2D circle -> square, 200 landmarks, the workload's 300-iteration budget (the
+    reference: 320 evaluations).  Not converged at this budget: the objective is
+    pinned to 1e-5, the landmarks to 2e-4 of the diameter (measured 1.2e-4); the
+    converged registration below carries the 1e-4 landmark criterion."""
     from lddmm_b200 import problem
 
     z = golden("circle2square_300")
+    P = problem.circle_to_square()
+    r, nde = _register(P, int(z["itr_max"]))
+    _check(P, z, r, nde, lm_tol=2e-4)
+
+
+def test_circle2square_converged_against_the_reference():
+    """2D circle -> square run to convergence (|g| < 1e-6; the reference needs ~18,000
+    evaluations).  At the 300-iteration budget both runs are still moving along a flat
+    valley (objective within 6e-6, landmarks ~1.2e-4 of the diameter apart); at the
+    minimum the landmark criterion applies.  The FP32 path may stop a little earlier
+    with the reference's code 3 at its noise floor."""
+    from lddmm_b200 import problem
+
+    z = golden("circle2square_converged")
     P = problem.circle_to_square()
     r, nde = _register(P, int(z["itr_max"]))
     _check(P, z, r, nde)

@@ -207,13 +207,15 @@ def test_lddmm_matlab_interface(api):
     assert np.all(np.isfinite(out.ndeStk))
 
 
-@pytest.mark.parametrize("persistent", [-1, 1])
+@pytest.mark.parametrize("persistent", [-1, 1, 2])
 def test_uneven_3d_batch_objgrd_equals_individual(api, persistent):
     """Uneven 3D surface pairs (star surfaces of 600-2600 vertices onto targets of
     1000-4000 triangles, as in the 256-pair population) evaluated in one batched
     context: every pair's objective and gradient equal its own single-pair
     evaluation with the same launch shape (per-step sweeps with one CTA per tile, or
-    the persistent sweeps), so batching changes nothing but the launches."""
+    the persistent sweeps in either form: split row groups combined through L2 (1) or
+    by thread-block clusters through distributed shared memory (2)), so batching
+    changes nothing but the launches."""
     from lddmm_b200 import problem
 
     probs = problem.population(n_pairs=4, seed=3, n_min=600, n_max=2600, t_min=1000,

@@ -156,8 +156,11 @@ int lddmm_ctx_launch_config(const lddmm_ctx *ctx, int *out3);
 /* Launch shape in use: out[0..2] cluster sizes (shoot, adjoint, varifold), out[3..4]
  * 64-row tiles per work item of the shooting / adjoint sweeps, out[5] the form of
  * the time loops (0 per-step launches, 1 persistent with L2 combine, 2 persistent
- * cluster form).  Returns 6. */
-int lddmm_ctx_launch_shape(const lddmm_ctx *ctx, int *out6);
+ * cluster form); the persistent plans: out[6] cluster size and out[7] CTAs of the
+ * cluster form (0: unavailable), out[8] CTAs of the L2 form, out[9] / out[10] the
+ * largest CTA share (j entries of 16 rows) of the cluster / L2 plan.  Writes at most n
+ * values; returns the number written. */
+int lddmm_ctx_launch_shape(const lddmm_ctx *ctx, int *out, int n);
 
 /* Objective and gradient of every pair at alp (concatenated, host memory);
  * fcn[num], grd like alp.  objgrd.cpp:26 semantics. */

@@ -88,7 +88,7 @@ def _load():
     L.lddmm_ctx_stream.argtypes = [C.c_void_p]
     L.lddmm_ctx_stream.restype = C.c_void_p
     L.lddmm_ctx_launch_config.argtypes = [C.c_void_p, _ip]
-    L.lddmm_ctx_launch_shape.argtypes = [C.c_void_p, _ip]
+    L.lddmm_ctx_launch_shape.argtypes = [C.c_void_p, _ip, C.c_int]
     L.lddmm_objgrd.argtypes = [C.c_void_p, _dp, _dp, _dp]
     L.lddmm_objgrd_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
     L.lddmm_lbfgs.argtypes = [C.c_void_p, C.POINTER(Opt), _dp, C.POINTER(Result)]

@@ -88,13 +88,18 @@ class Context:
 
     def launch_shape(self):
         """dict(cluster=(shoot, adjoint, varifold), tiles=(shoot, adjoint),
-        persistent=0 | 1 | 2): the launch shape the context runs (after autotuning);
-        persistent 0: per-step launches, 1: persistent time loops combining split row
-        groups in L2, 2: the cluster form."""
-        o = np.zeros(6, dtype=np.int32)
-        check(lib.lddmm_ctx_launch_shape(self._h, iptr(o)))
+        persistent=0 | 1 | 2, plans=...): the launch shape the context runs (after
+        autotuning); persistent 0: per-step launches, 1: persistent time loops
+        combining split row groups in L2, 2: the cluster form.  plans: the cluster
+        form's cluster size and CTAs, the L2 form's CTAs, and each plan's largest CTA
+        share."""
+        o = np.zeros(11, dtype=np.int32)
+        check(lib.lddmm_ctx_launch_shape(self._h, iptr(o), 11))
         return dict(cluster=tuple(int(x) for x in o[:3]), tiles=(int(o[3]), int(o[4])),
-                    persistent=int(o[5]))
+                    persistent=int(o[5]),
+                    plans=dict(cluster_size=int(o[6]), cluster_ctas=int(o[7]),
+                               l2_ctas=int(o[8]), cluster_share=int(o[9]),
+                               l2_share=int(o[10])))
 
     def time_sweeps(self, reps=3):
         """Average ms per launch: shooting step, adjoint step, varifold sweep, and

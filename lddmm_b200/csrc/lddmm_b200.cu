@@ -1358,15 +1358,14 @@ extern "C" int lddmm_ctx_launch_config(const lddmm_ctx *c, int *o) {
   return 0;
 }
 
-extern "C" int lddmm_ctx_launch_shape(const lddmm_ctx *c, int *o) {
-  if (!c || !o) return LDDMM_ERR_ARG;
-  o[0] = c->S_shoot;
-  o[1] = c->S_adj;
-  o[2] = c->S_vfd;
-  o[3] = c->tpw_shoot;
-  o[4] = c->tpw_adj;
-  o[5] = c->persistent ? 1 + c->pers_kind : 0;
-  return 6;
+extern "C" int lddmm_ctx_launch_shape(const lddmm_ctx *c, int *o, int n) {
+  if (!c || !o || n < 0) return LDDMM_ERR_ARG;
+  const long long v[11] = {c->S_shoot, c->S_adj, c->S_vfd, c->tpw_shoot, c->tpw_adj,
+                           c->persistent ? 1 + c->pers_kind : 0, c->pers_C, c->pers_cl_ctas,
+                           c->pers_ctas, c->pers_cl_share, c->pers_l2_share};
+  const int k = std::min(n, 11);
+  for (int i = 0; i < k; ++i) o[i] = (int)v[i];
+  return k;
 }
 
 // ================================================================ objective

@@ -518,7 +518,11 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 2)
     if (job.x >= 0) {
       // the parts of the split row group whose first part this CTA holds
       const int2 un = plan.units[job.x];
-      const int job_pair = un.x, job_grp = un.y;
+      const int job_pair = un.x, job_grp = un.y, row = job_grp * kGroup + lane;
+      Op &oj = o;
+      oj.pd = op.pd;  // global descriptors (the rounds pointed o.pd at the round slots)
+      typename Op::FData F;  // finalize operands, in flight during the wait
+      if (lane < kGroup) oj.fin_load(job_pair, row, F);
       unsigned int n = 0;
       bool ok = true;
       while (!mbar_test_parity(&s_bar, (unsigned int)(s & 1))) {
@@ -532,12 +536,7 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 2)
         }
       }
       ok = __all_sync(0xffffffffu, ok);
-      Op &oj = o;
-      oj.pd = op.pd;  // global descriptors (the rounds pointed o.pd at the round slots)
       if (ok && lane < kGroup && oj.active(job_pair)) {
-        const int row = job_grp * kGroup + lane;
-        typename Op::FData F;
-        oj.fin_load(job_pair, row, F);
         double v[NA];
 #pragma unroll
         for (int a = 0; a < NA; ++a) v[a] = 0.0;

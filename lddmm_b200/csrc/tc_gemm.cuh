@@ -22,6 +22,7 @@
 // (tcgen05 "Shared memory descriptor", "Instruction descriptor" for kind::f16).
 #pragma once
 
+#include <cuda.h>  // CUtensorMap (the map is encoded on the host, see warmstart.cu)
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -160,13 +161,15 @@ __device__ __forceinline__ void stage_async(unsigned char *dst, const __nv_bfloa
   }
 }
 
-// Epilogue of one 128-row tile: the accumulator (TMEM, warp w owns lanes 32w..32w+31
-// = rows m0 + 32w ..) through bias / GELU / GELU' into the outputs of `g`; `out` is the
-// FP32 output of this K split (or null).  Called by all 4 warps after the tile's MMAs
-// completed and tcgen05.fence::after_thread_sync.
+// Epilogue of one 128-row tile: the accumulator (TMEM; the calling warp reads lane
+// quadrant `quad`, lanes 32 quad .. 32 quad + 31 = rows m0 + 32 quad ..; a warp may
+// only access the quadrant of its warp index mod 4) through bias / GELU / GELU' into
+// the outputs of `g`; `out` is the FP32 output of this K split (or null).  Called by
+// four warps covering the four quadrants after the tile's MMAs completed and
+// tcgen05.fence::after_thread_sync.
 __device__ __forceinline__ void gemm_epilogue(const GemmArgs &g, int m0, uint32_t tmem,
-                                              float *out) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+                                              float *out, int quad) {
+  const int warp = quad, lane = threadIdx.x & 31;
   const int m = m0 + warp * 32 + lane;
   const bool row_ok = m < g.M;
   // four columns per store where every output in use allows it
@@ -326,7 +329,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_bf16_kernel(GemmArgs g) 
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (s_ok && issued > 0)
-    gemm_epilogue(g, m0, tmem, g.out ? g.out + (size_t)blockIdx.y * g.split_stride : nullptr);
+    gemm_epilogue(g, m0, tmem, g.out ? g.out + (size_t)blockIdx.y * g.split_stride : nullptr,
+                  warp);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
@@ -431,7 +435,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) gemm_bf16_resident_kernel(Gem
       __syncthreads();
       if (!s_ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      gemm_epilogue(g, (blockIdx.x + (q / nk) * gridDim.x) * kTileM, tmem, g.out);
+      gemm_epilogue(g, (blockIdx.x + (q / nk) * gridDim.x) * kTileM, tmem, g.out, warp);
       // the next tile's first MMA overwrites the accumulator
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncthreads();
@@ -452,6 +456,187 @@ inline size_t gemm_resident_smem_bytes(int N, int K) {
 
 // Dynamic shared memory of gemm_bf16_kernel for N columns (two stage buffers).
 inline size_t gemm_smem_bytes(int N) { return 2 * (size_t)(kTileM + N) * kKC * 2; }
+
+// ---------------------------------------------------------------------------------
+// Warp-specialised weight-resident form (one K split, K <= kResK, N <= 256): the
+// layers of the warm-start network move ~250 MB per hidden-layer product and do
+// little arithmetic per byte, so the kernel is built to keep HBM busy: loads, MMAs and
+// the epilogue of different tiles overlap.  One persistent CTA per SM, 6 warps:
+//   warp 0   producer: the weights once, then the A chunks of its tiles, by TMA
+//            (cp.async.bulk.tensor, no multicast: this GPU's memory only), into
+//            kWsStages stage buffers; a buffer is refilled after the MMAs reading it
+//            have committed to its "empty" mbarrier;
+//   warp 1   MMA issuer (one thread): tcgen05.mma into one of two TMEM accumulators
+//            (tile i uses accumulator i & 1), commit to the buffer's "empty" barrier
+//            per chunk and to the accumulator's "full" barrier per tile;
+//   warps 2-5 epilogue: tile i's accumulator through gemm_epilogue (warp w reads TMEM
+//            lane quadrant w & 3) while tile i + 1 accumulates into the other one,
+//            then release it on its "empty" barrier.
+// TMA writes each box of 8 K-elements x rows as rows x 16 bytes, so a stage of A
+// (128 rows x kKC) is 8 boxes at 2 KB strides: the canonical K-major layout without
+// swizzle with the leading byte offset (next 8 K-elements) 2048 and the stride byte
+// offset (next 8 rows) 128; the weights likewise with N x 16-byte boxes.  Out-of-range
+// rows and K elements are zero-filled by the TMA unit.  Every mbarrier wait is bounded
+// (error word); before freeing TMEM the producer waits (bounded) for its loads in
+// flight and the MMA thread for its last MMAs.
+constexpr int kWsStages = 4;
+constexpr int kWsThreads = 192;
+
+__device__ __forceinline__ void mbar_init_n(uint64_t *mbar, uint32_t n) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(n));
+}
+
+__device__ __forceinline__ void mbar_arrive1(uint64_t *mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(mbar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// TMA load of the box at (x = K element, y = row) of a 2D tensor map into dst.  x is a
+// multiple of 8 elements (16 bytes).
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
+                                            uint64_t *mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(smem_u32(mbar))
+      : "memory");
+}
+
+inline size_t gemm_ws_smem_bytes(int N, int K) {
+  const int nk = (K + kKC - 1) / kKC;
+  return (size_t)nk * kKC * N * 2 + (size_t)kWsStages * kTileM * kKC * 2;
+}
+
+__global__ void __launch_bounds__(kWsThreads, 1)
+    gemm_bf16_ws_kernel(GemmArgs g, const __grid_constant__ CUtensorMap tmA,
+                        const __grid_constant__ CUtensorMap tmB) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  __shared__ uint64_t s_full[kWsStages], s_empty[kWsStages], s_accf[2], s_acce[2], s_bfull,
+      s_mdone;
+  __shared__ uint32_t s_tmem;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nk = (g.K + kKC - 1) / kKC;
+  const uint32_t b_group = (uint32_t)g.N * 16;  // bytes of one 8-element K group of B
+  unsigned char *sB = smem;
+  unsigned char *sA = smem + (size_t)nk * 8 * b_group;
+  constexpr uint32_t kStageBytes = kTileM * kKC * 2;
+  const int ntiles = (g.M + kTileM - 1) / kTileM;
+  const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const uint32_t nacc = g.N <= 32 ? 32u : g.N <= 64 ? 64u : g.N <= 128 ? 128u : 256u;
+  const uint32_t ncols = 2 * nacc;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < kWsStages; ++b) {
+      mbar_init_n(&s_full[b], 1);
+      mbar_init_n(&s_empty[b], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init_n(&s_accf[b], 1);
+      mbar_init_n(&s_acce[b], 4);  // one arrival per epilogue warp
+    }
+    mbar_init_n(&s_bfull, 1);
+    mbar_init_n(&s_mdone, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+  auto fail = [&]() {
+    if (g.error) atomicExch(g.error, 1u);
+  };
+  const int Q = my_tiles * nk;  // (tile, K chunk) steps of this CTA
+  if (warp == 0) {
+    if (lane == 0) {
+      mbar_expect_tx(&s_bfull, (uint32_t)nk * 8 * b_group);
+      for (int c = 0; c < nk * 8; ++c) tma_load_2d(sB + (size_t)c * b_group, &tmB, c * 8, 0, &s_bfull);
+      int q = 0;
+      for (; q < Q; ++q) {
+        const int st = q % kWsStages;
+        if (!mbar_wait(&s_empty[st], (uint32_t)(((q / kWsStages) & 1) ^ 1))) {
+          fail();
+          break;
+        }
+        mbar_expect_tx(&s_full[st], kStageBytes);
+        const int row = (blockIdx.x + (q / nk) * gridDim.x) * kTileM;
+        const int k0 = (q % nk) * kKC;
+        unsigned char *dst = sA + (size_t)st * kStageBytes;
+        for (int c = 0; c < kKC / 8; ++c)
+          tma_load_2d(dst + c * (kTileM * 16), &tmA, k0 + c * 8, row, &s_full[st]);
+      }
+      // the loads in flight complete before the CTA leaves (bounded)
+      for (int r = (q > kWsStages ? q - kWsStages : 0); r < q; ++r)
+        if (!mbar_wait(&s_full[r % kWsStages], (uint32_t)((r / kWsStages) & 1))) fail();
+      if (!mbar_wait(&s_bfull, 0u)) fail();
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t idesc = instr_desc_bf16(kTileM, g.N);
+      bool ok = mbar_wait(&s_bfull, 0u);
+      if (!ok) fail();
+      for (int i = 0; ok && i < my_tiles; ++i) {
+        const int acc = i & 1;
+        if (!mbar_wait(&s_acce[acc], (uint32_t)(((i >> 1) & 1) ^ 1))) {
+          fail();
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t d = tmem + (uint32_t)acc * nacc;
+        for (int kc = 0; kc < nk; ++kc) {
+          const int q = i * nk + kc, st = q % kWsStages;
+          if (!mbar_wait(&s_full[st], (uint32_t)((q / kWsStages) & 1))) {
+            fail();
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a0 = smem_u32(sA + (size_t)st * kStageBytes);
+          const uint32_t b0 = smem_u32(sB + (size_t)kc * 8 * b_group);
+#pragma unroll
+          for (int s = 0; s < kKC / 16; ++s) {
+            const uint64_t da = smem_desc(a0 + s * 2 * (kTileM * 16), kTileM * 16, 128);
+            const uint64_t db = smem_desc(b0 + s * 2 * b_group, b_group, 128);
+            mma_bf16(d, da, db, idesc, (kc == 0 && s == 0) ? 0u : 1u);
+          }
+          mma_commit(&s_empty[st]);
+        }
+        if (ok) mma_commit(&s_accf[acc]);
+      }
+      // every MMA issued has completed before TMEM is freed (bounded)
+      mma_commit(&s_mdone);
+      if (!mbar_wait(&s_mdone, 0u)) fail();
+    }
+  } else {
+    const int quad = warp & 3;  // TMEM lane quadrant this warp may read
+    for (int i = 0; i < my_tiles; ++i) {
+      const int acc = i & 1;
+      if (!mbar_wait(&s_accf[acc], (uint32_t)((i >> 1) & 1))) {
+        fail();
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      gemm_epilogue(g, (blockIdx.x + i * gridDim.x) * kTileM, tmem + (uint32_t)acc * nacc, g.out,
+                    quad);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive1(&s_acce[acc]);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+}
 
 }  // namespace tc
 }  // namespace lddmm

@@ -26,6 +26,7 @@
 // Every reduction runs in a fixed order, so training is bit-reproducible.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <atomic>
@@ -34,6 +35,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -342,10 +344,45 @@ cudaError_t refresh_bf16(lddmm_ws &w) {
   return cudaGetLastError();
 }
 
-// Launches C = A . B^T on `st`: the weight-resident persistent kernel when there is one
-// K split with K <= kResK (every layer's forward and input-gradient products), else
-// the per-tile kernel (split-K weight gradients).  Both kernels' shared-memory limits
-// are raised once per device.
+// cuTensorMapEncodeTiled from the driver, looked up once through the runtime (the
+// library does not link the driver library itself); null when unavailable.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// 2D TMA map of a K-major BF16 matrix (rows x K, row stride ld elements) read in boxes
+// of 8 K-elements x box_rows rows; false when the operand does not meet TMA's rules
+// (16-byte aligned base and row stride) or the encoder refuses it.
+bool make_kmajor_map(CUtensorMap *m, const void *base, long long K, long long rows,
+                     long long ld, int box_rows) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || ((uintptr_t)base & 15u) || (ld * 2) % 16 || K < 8 || rows < 1) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+  cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1u, 1u};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides,
+             box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+// Launches C = A . B^T on `st`.  One K split with K <= kResK (every layer's forward and
+// input-gradient products): the warp-specialised TMA kernel, or the cp.async
+// weight-resident kernel when TMA maps cannot be made for the operands; otherwise the
+// per-tile kernel (split-K weight gradients).  The kernels' shared-memory limits are
+// raised once per device.
 cudaError_t launch_gemm(GemmArgs a, int splits, cudaStream_t st) {
   static std::atomic<bool> attr_set[64];  // zero-initialised; setting twice is harmless
   int dev = 0;
@@ -358,6 +395,9 @@ cudaError_t launch_gemm(GemmArgs a, int splits, cudaStream_t st) {
       e = cudaFuncSetAttribute(gemm_bf16_resident_kernel,
                                cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)gemm_resident_smem_bytes(256, kResK));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(gemm_bf16_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)gemm_ws_smem_bytes(256, kResK));
     if (e != cudaSuccess) return e;
     attr_set[dev].store(true);
   }
@@ -367,7 +407,12 @@ cudaError_t launch_gemm(GemmArgs a, int splits, cudaStream_t st) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = std::min(ntiles, std::max(sms, 1));
-    gemm_bf16_resident_kernel<<<grid, kGemmThreads, gemm_resident_smem_bytes(a.N, a.K), st>>>(a);
+    CUtensorMap ma, mb;
+    if (make_kmajor_map(&ma, a.A, a.K, a.M, a.lda, kTileM) &&
+        make_kmajor_map(&mb, a.B, a.K, a.N, a.ldb, a.N))
+      gemm_bf16_ws_kernel<<<grid, kWsThreads, gemm_ws_smem_bytes(a.N, a.K), st>>>(a, ma, mb);
+    else
+      gemm_bf16_resident_kernel<<<grid, kGemmThreads, gemm_resident_smem_bytes(a.N, a.K), st>>>(a);
   } else {
     gemm_bf16_kernel<<<dim3(ntiles, splits), kGemmThreads, gemm_smem_bytes(a.N), st>>>(a);
   }

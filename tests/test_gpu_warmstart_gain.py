@@ -1,16 +1,24 @@
 """What the trained warm-start network gains over the plain method, end to end at a
 reduced size (642-landmark icosphere onto 1280-triangle perturbed spheres, T = 10):
 1024 plain-method registrations train the network (400 epochs), then 32 held-out
-pairs are registered from zero and from the prediction.  The prediction must start L-BFGS at a
-clearly lower objective, and the plain method, run to convergence from it, must reach
-the cold start's objective (the result is judged by the plain method, not by the
-network)."""
+pairs are registered from zero (cold) and from the prediction (warm), both run to
+convergence (relative objective change below 1e-9, at most 1000 iterations).
+
+Measured and asserted, per held-out pair:
+  * time to tolerance: objective evaluations (and batch wall time) until the run is
+    within 1e-5 relative of the cold start's converged objective; the medians of warm
+    and cold are reported, and the warm start must not be slower;
+  * the result is judged by the plain method, not by the network: the warm run's
+    converged objective must match the cold start's within 1e-5 relative.
+The prediction must also start L-BFGS at a clearly lower objective."""
 import functools
 
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+REL = 1e-5
 
 
 def test_warm_start_gain():
@@ -22,13 +30,22 @@ def test_warm_start_gain():
     with W.WarmStart(src, W.T_STEPS, batch_max=64, tri_max=tri.shape[1], label_scale=scale,
                      seed=0) as ws:
         hist = W.train(ws, tri, lab, epochs=400, batch=64, lr=1e-3)
-        ev = W.evaluate(ws, list(range(50000, 50032)), batch=32, make=make)
+        ev = W.evaluate(ws, list(range(50000, 50032)), batch=32, make=make, itr_max=1000,
+                        rel_obj_tol=1e-9, rel=REL)
     rows = ev["rows"]
     ratio = np.median([r["f_start_warm"] / r["f_start_cold"] for r in rows])
+    dev = np.array([abs(r["f_warm"] - r["f_cold"]) / abs(r["f_cold"]) for r in rows])
+    print(f"time to tolerance (median evaluations): cold {ev['median_evals_cold']}, warm "
+          f"{ev['median_evals_warm']}, median per-pair gain {ev['median_speedup_evals']:.2f}x; "
+          f"wall {ev['seconds_cold']:.2f} s cold, {ev['seconds_warm']:.2f} s warm; start "
+          f"objective ratio {ratio:.3f}; converged objectives within {REL:g}: "
+          f"{int(np.sum(dev <= REL))}/{len(rows)} (median deviation {np.median(dev):.2e})")
     assert hist[-1] < 0.8 * hist[0], hist[::10]
     assert ratio < 0.8, ratio
-    # converged objectives: the typical warm run ends within 1e-4 of the cold start's
-    # (this non-convex problem's runs from different starts stop ~1e-5 apart)
-    dev = [abs(r["f_warm"] - r["f_cold"]) / abs(r["f_cold"]) for r in rows]
-    assert np.median(dev) <= 1e-4, np.median(dev)
     assert all(r["f_warm"] == r["f_warm"] for r in rows)
+    # judged by the plain method: converged objectives agree within 1e-5
+    assert np.median(dev) <= REL, np.median(dev)
+    assert np.mean(dev <= REL) >= 0.9, dev
+    # time to tolerance: the warm start is not slower than the cold start
+    assert ev["reached"] >= 0.9 * len(rows)
+    assert ev["median_evals_warm"] <= ev["median_evals_cold"], ev

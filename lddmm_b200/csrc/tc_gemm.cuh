@@ -507,9 +507,13 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
+// Dynamic shared memory of gemm_bf16_ws_kernel: the weights and the A stages, and at
+// least 120 KB, so that one CTA runs per SM and its two accumulators (up to 512 TMEM
+// columns) never compete with another CTA's for the SM's tensor memory.
 inline size_t gemm_ws_smem_bytes(int N, int K) {
   const int nk = (K + kKC - 1) / kKC;
-  return (size_t)nk * kKC * N * 2 + (size_t)kWsStages * kTileM * kKC * 2;
+  const size_t need = (size_t)nk * kKC * N * 2 + (size_t)kWsStages * kTileM * kKC * 2;
+  return need > (size_t)120 * 1024 ? need : (size_t)120 * 1024;
 }
 
 __global__ void __launch_bounds__(kWsThreads, 1)

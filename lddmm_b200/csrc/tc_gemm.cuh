@@ -476,11 +476,19 @@ inline size_t gemm_smem_bytes(int N) { return 2 * (size_t)(kTileM + N) * kKC * 2
 // (128 rows x kKC) is 8 boxes at 2 KB strides: the canonical K-major layout without
 // swizzle with the leading byte offset (next 8 K-elements) 2048 and the stride byte
 // offset (next 8 rows) 128; the weights likewise with N x 16-byte boxes.  Out-of-range
-// rows and K elements are zero-filled by the TMA unit.  Every mbarrier wait is bounded
-// (error word); before freeing TMEM the producer waits (bounded) for its loads in
-// flight and the MMA thread for its last MMAs.
-constexpr int kWsStages = 4;
+// rows and K elements are zero-filled by the TMA unit.
+// A plain FP32 output (no activation, at most a bias) leaves through TMA stores: each
+// epilogue warp writes its 32 rows x 32 columns into one of two 4 KB staging buffers
+// in the 128-byte swizzled layout (16-byte chunk k of row r at chunk k ^ (r & 7):
+// conflict-free) and one lane stores the block with cp.async.bulk.tensor, so HBM sees
+// whole 128-byte rows instead of one 16-byte piece per row per instruction; a buffer
+// is rewritten after the store that read it (bulk wait_group.read).  Every mbarrier
+// wait is bounded (error word); before freeing TMEM the producer waits (bounded) for
+// its loads in flight, the MMA thread for its last MMAs and the epilogue lanes for
+// their stores.
+constexpr int kWsMaxStages = 4;
 constexpr int kWsThreads = 192;
+constexpr int kWsStageC = 32 * 32 * 4;  // one epilogue staging buffer (bytes)
 
 __device__ __forceinline__ void mbar_init_n(uint64_t *mbar, uint32_t n) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(mbar)), "r"(n));
@@ -494,6 +502,17 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *mbar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(mbar)),
                "r"(bytes)
                : "memory");
+}
+
+// TMA store of the box at (x = column, y = row) of a 2D tensor map from src (bulk
+// group of the calling thread).  x is a multiple of 4 FP32 columns (16 bytes), y >= 0.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, int x, int y,
+                                             const void *src) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(map),
+      "r"(x), "r"(y), "r"(smem_u32(src))
+      : "memory");
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
 }
 
 // TMA load of the box at (x = K element, y = row) of a 2D tensor map into dst.  x is a
@@ -510,25 +529,78 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
 // Dynamic shared memory of gemm_bf16_ws_kernel: the weights and the A stages, and at
 // least 120 KB, so that one CTA runs per SM and its two accumulators (up to 512 TMEM
 // columns) never compete with another CTA's for the SM's tensor memory.
-inline size_t gemm_ws_smem_bytes(int N, int K) {
+// A stages of gemm_bf16_ws_kernel that fit next to the weights (and the epilogue
+// staging buffers when the output leaves through TMA stores): up to kWsMaxStages,
+// at least 2.
+inline int gemm_ws_stages(int N, int K, bool tma_store) {
   const int nk = (K + kKC - 1) / kKC;
-  const size_t need = (size_t)nk * kKC * N * 2 + (size_t)kWsStages * kTileM * kKC * 2;
+  const size_t fixed = (size_t)nk * kKC * N * 2 + (tma_store ? 8 * kWsStageC + 1024 : 0) + 1024;
+  const size_t cap = 227 * 1024 - 1024;  // the per-CTA limit less the static barriers
+  int st = kWsMaxStages;
+  while (st > 2 && fixed + (size_t)st * kTileM * kKC * 2 > cap) --st;
+  return st;
+}
+
+inline size_t gemm_ws_smem_bytes(int N, int K, bool tma_store) {
+  const int nk = (K + kKC - 1) / kKC;
+  const size_t need = (size_t)nk * kKC * N * 2 +
+                      (size_t)gemm_ws_stages(N, K, tma_store) * kTileM * kKC * 2 +
+                      (tma_store ? 8 * kWsStageC + 1024 : 0);
   return need > (size_t)120 * 1024 ? need : (size_t)120 * 1024;
+}
+
+// Epilogue of one 128-row tile through TMA stores (plain FP32 output, optional bias):
+// warp quadrant `quad`, rows m0 + 32 quad + lane, 32 columns per block.  `cstage`: the
+// warp's two staging buffers (1024-byte aligned); `nst`: stores issued so far by this
+// warp (selects the buffer).
+__device__ __forceinline__ void gemm_epilogue_tma(const GemmArgs &g, const CUtensorMap *tmC,
+                                                  int m0, uint32_t tmem, int quad,
+                                                  unsigned char *cstage, int &nst) {
+  const int lane = threadIdx.x & 31;
+  const int row0 = m0 + quad * 32;
+  for (int c0 = 0; c0 < g.n_valid; c0 += 32) {
+    float v[32];
+    tmem_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
+    if (row0 >= g.M) continue;  // a quadrant wholly below the matrix stores nothing
+    if (g.bias) {
+#pragma unroll
+      for (int j = 0; j < 32; ++j)
+        if (c0 + j < g.n_valid) v[j] += g.bias[c0 + j];
+    }
+    unsigned char *buf = cstage + (nst & 1) * kWsStageC;
+    if (nst >= 2 && lane == 0)  // the store that read this buffer has read it
+      asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      *reinterpret_cast<float4 *>(buf + lane * 128 + ((k ^ (lane & 7)) << 4)) =
+          make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncwarp();
+    if (lane == 0) tma_store_2d(tmC, c0, row0, buf);
+    ++nst;
+  }
 }
 
 __global__ void __launch_bounds__(kWsThreads, 1)
     gemm_bf16_ws_kernel(GemmArgs g, const __grid_constant__ CUtensorMap tmA,
-                        const __grid_constant__ CUtensorMap tmB) {
+                        const __grid_constant__ CUtensorMap tmB,
+                        const __grid_constant__ CUtensorMap tmC, int tma_store, int stages) {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ uint64_t s_full[kWsStages], s_empty[kWsStages], s_accf[2], s_acce[2], s_bfull,
-      s_mdone;
+  __shared__ uint64_t s_full[kWsMaxStages], s_empty[kWsMaxStages], s_accf[2], s_acce[2],
+      s_bfull, s_mdone;
   __shared__ uint32_t s_tmem;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nk = (g.K + kKC - 1) / kKC;
   const uint32_t b_group = (uint32_t)g.N * 16;  // bytes of one 8-element K group of B
+  const int kWsStages = stages;  // A stage buffers (<= kWsMaxStages)
   unsigned char *sB = smem;
   unsigned char *sA = smem + (size_t)nk * 8 * b_group;
   constexpr uint32_t kStageBytes = kTileM * kKC * 2;
+  // epilogue staging buffers, 1024-byte aligned (the 128-byte swizzle repeats every
+  // 8 rows of 128 bytes)
+  const uint32_t c_off = (uint32_t)((size_t)nk * 8 * b_group + (size_t)stages * kStageBytes);
+  unsigned char *sC = smem + c_off + ((1024u - ((smem_u32(smem) + c_off) & 1023u)) & 1023u);
   const int ntiles = (g.M + kTileM - 1) / kTileM;
   const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const uint32_t nacc = g.N <= 32 ? 32u : g.N <= 64 ? 64u : g.N <= 128 ? 128u : 256u;
@@ -622,6 +694,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     }
   } else {
     const int quad = warp & 3;  // TMEM lane quadrant this warp may read
+    unsigned char *cstage = sC + (size_t)(warp - 2) * 2 * kWsStageC;
+    int nst = 0;  // TMA stores issued by this warp
     for (int i = 0; i < my_tiles; ++i) {
       const int acc = i & 1;
       if (!mbar_wait(&s_accf[acc], (uint32_t)((i >> 1) & 1))) {
@@ -629,12 +703,18 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      gemm_epilogue(g, (blockIdx.x + i * gridDim.x) * kTileM, tmem + (uint32_t)acc * nacc, g.out,
-                    quad);
+      const int m0 = (blockIdx.x + i * gridDim.x) * kTileM;
+      if (tma_store)
+        gemm_epilogue_tma(g, &tmC, m0, tmem + (uint32_t)acc * nacc, quad, cstage, nst);
+      else
+        gemm_epilogue(g, m0, tmem + (uint32_t)acc * nacc, g.out, quad);
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive1(&s_acce[acc]);
     }
+    // the stores have finished before the CTA leaves
+    if (lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    __syncwarp();
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();

@@ -378,6 +378,21 @@ bool make_kmajor_map(CUtensorMap *m, const void *base, long long K, long long ro
          CUDA_SUCCESS;
 }
 
+// 2D TMA map of a row-major FP32 output (rows x cols, row stride ld elements) written
+// in 32 x 32 blocks through a 128-byte-swizzled staging buffer; false when the output
+// does not meet TMA's rules (16-byte aligned base and row stride).
+bool make_out_map(CUtensorMap *m, float *base, long long cols, long long rows, long long ld) {
+  const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc || ((uintptr_t)base & 15u) || (ld * 4) % 16 || cols < 4 || rows < 1) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
+  cuuint32_t box[2] = {32u, 32u};
+  cuuint32_t es[2] = {1u, 1u};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // Launches C = A . B^T on `st`.  One K split with K <= kResK (every layer's forward and
 // input-gradient products): the warp-specialised TMA kernel, or the cp.async
 // weight-resident kernel when TMA maps cannot be made for the operands; otherwise the
@@ -397,7 +412,8 @@ cudaError_t launch_gemm(GemmArgs a, int splits, cudaStream_t st) {
                                (int)gemm_resident_smem_bytes(256, kResK));
     if (e == cudaSuccess)
       e = cudaFuncSetAttribute(gemm_bf16_ws_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)gemm_ws_smem_bytes(256, kResK));
+                               (int)std::max(gemm_ws_smem_bytes(256, kResK, true),
+                                             gemm_ws_smem_bytes(256, kResK, false)));
     if (e != cudaSuccess) return e;
     attr_set[dev].store(true);
   }
@@ -407,11 +423,16 @@ cudaError_t launch_gemm(GemmArgs a, int splits, cudaStream_t st) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = std::min(ntiles, std::max(sms, 1));
-    CUtensorMap ma, mb;
+    CUtensorMap ma, mb, mc;
+    std::memset(&mc, 0, sizeof(mc));
     if (make_kmajor_map(&ma, a.A, a.K, a.M, a.lda, kTileM) &&
-        make_kmajor_map(&mb, a.B, a.K, a.N, a.ldb, a.N))
-      gemm_bf16_ws_kernel<<<grid, kWsThreads, gemm_ws_smem_bytes(a.N, a.K), st>>>(a, ma, mb);
-    else
+        make_kmajor_map(&mb, a.B, a.K, a.N, a.ldb, a.N)) {
+      // a plain FP32 output leaves through TMA stores
+      const bool tma_store = a.out && a.epi == kEpiNone && !a.pre_out && !a.out_bf &&
+                             !a.out_bt && make_out_map(&mc, a.out, a.n_valid, a.M, a.ldo);
+      gemm_bf16_ws_kernel<<<grid, kWsThreads, gemm_ws_smem_bytes(a.N, a.K, tma_store), st>>>(
+          a, ma, mb, mc, tma_store ? 1 : 0, gemm_ws_stages(a.N, a.K, tma_store));
+    } else
       gemm_bf16_resident_kernel<<<grid, kGemmThreads, gemm_resident_smem_bytes(a.N, a.K), st>>>(a);
   } else {
     gemm_bf16_kernel<<<dim3(ntiles, splits), kGemmThreads, gemm_smem_bytes(a.N), st>>>(a);

@@ -121,6 +121,23 @@ __device__ __forceinline__ float gelu_grad(float x) {
          x * 0.39894228040143268f * __expf(-0.5f * x * x);
 }
 
+// 32 consecutive accumulator columns of this thread's TMEM lane, without waiting for
+// the load (tcgen05.wait::ld before the registers are read).
+__device__ __forceinline__ void tmem_ld32_async(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+      "[%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(taddr));
+}
+
 // 32 consecutive accumulator columns of this thread's TMEM lane.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   uint32_t r[32];
@@ -558,27 +575,40 @@ __device__ __forceinline__ void gemm_epilogue_tma(const GemmArgs &g, const CUten
                                                   unsigned char *cstage, int &nst) {
   const int lane = threadIdx.x & 31;
   const int row0 = m0 + quad * 32;
-  for (int c0 = 0; c0 < g.n_valid; c0 += 32) {
-    float v[32];
-    tmem_ld32(tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)c0, v);
+  const uint32_t tq = tmem + ((uint32_t)(quad * 32) << 16);
+  // two 32-column blocks per TMEM round trip
+  for (int c0 = 0; c0 < g.n_valid; c0 += 64) {
+    const bool two = c0 + 32 < g.n_valid;
+    uint32_t r[2][32];
+    tmem_ld32_async(tq + (uint32_t)c0, r[0]);
+    if (two) tmem_ld32_async(tq + (uint32_t)(c0 + 32), r[1]);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
     if (row0 >= g.M) continue;  // a quadrant wholly below the matrix stores nothing
-    if (g.bias) {
 #pragma unroll
-      for (int j = 0; j < 32; ++j)
-        if (c0 + j < g.n_valid) v[j] += g.bias[c0 + j];
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && !two) break;
+      const int cb = c0 + 32 * h;
+      float v[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[h][j]);
+      if (g.bias) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+          if (cb + j < g.n_valid) v[j] += g.bias[cb + j];
+      }
+      unsigned char *buf = cstage + (nst & 1) * kWsStageC;
+      if (nst >= 2 && lane == 0)  // the store that read this buffer has read it
+        asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        *reinterpret_cast<float4 *>(buf + lane * 128 + ((k ^ (lane & 7)) << 4)) =
+            make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) tma_store_2d(tmC, cb, row0, buf);
+      ++nst;
     }
-    unsigned char *buf = cstage + (nst & 1) * kWsStageC;
-    if (nst >= 2 && lane == 0)  // the store that read this buffer has read it
-      asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
-    __syncwarp();
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-      *reinterpret_cast<float4 *>(buf + lane * 128 + ((k ^ (lane & 7)) << 4)) =
-          make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncwarp();
-    if (lane == 0) tma_store_2d(tmC, c0, row0, buf);
-    ++nst;
   }
 }
 

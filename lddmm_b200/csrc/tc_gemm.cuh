@@ -185,7 +185,8 @@ __device__ __forceinline__ void stage_async(unsigned char *dst, const __nv_bfloa
 // four warps covering the four quadrants after the tile's MMAs completed and
 // tcgen05.fence::after_thread_sync.
 __device__ __forceinline__ void gemm_epilogue(const GemmArgs &g, int m0, uint32_t tmem,
-                                              float *out, int quad) {
+                                              float *out, int quad, int cbeg = 0,
+                                              int cend = 1 << 30) {
   const int warp = quad, lane = threadIdx.x & 31;
   const int m = m0 + warp * 32 + lane;
   const bool row_ok = m < g.M;
@@ -196,7 +197,7 @@ __device__ __forceinline__ void gemm_epilogue(const GemmArgs &g, int m0, uint32_
       (!g.out_bf || (((uintptr_t)g.out_bf & 7u) == 0 && (g.ldb_out & 3) == 0)) &&
       (g.epi != kEpiDGelu ||
        (((uintptr_t)g.pre_in & 15u) == 0 && (g.ld_pre_in & 3) == 0));
-  for (int c0 = 0; c0 < g.N; c0 += 32) {
+  for (int c0 = cbeg; c0 < g.N && c0 < cend; c0 += 32) {
     float v[32];
     tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
     if (!row_ok) continue;
@@ -478,7 +479,7 @@ inline size_t gemm_smem_bytes(int N) { return 2 * (size_t)(kTileM + N) * kKC * 2
 // Warp-specialised weight-resident form (one K split, K <= kResK, N <= 256): the
 // layers of the warm-start network move ~250 MB per hidden-layer product and do
 // little arithmetic per byte, so the kernel is built to keep HBM busy: loads, MMAs and
-// the epilogue of different tiles overlap.  One persistent CTA per SM, 6 warps:
+// the epilogue of different tiles overlap.  One persistent CTA per SM, 10 warps:
 //   warp 0   producer: the weights once, then the A chunks of its tiles, by TMA
 //            (cp.async.bulk.tensor, no multicast: this GPU's memory only), into
 //            kWsStages stage buffers; a buffer is refilled after the MMAs reading it
@@ -486,25 +487,29 @@ inline size_t gemm_smem_bytes(int N) { return 2 * (size_t)(kTileM + N) * kKC * 2
 //   warp 1   MMA issuer (one thread): tcgen05.mma into one of two TMEM accumulators
 //            (tile i uses accumulator i & 1), commit to the buffer's "empty" barrier
 //            per chunk and to the accumulator's "full" barrier per tile;
-//   warps 2-5 epilogue: tile i's accumulator through gemm_epilogue (warp w reads TMEM
-//            lane quadrant w & 3) while tile i + 1 accumulates into the other one,
-//            then release it on its "empty" barrier.
+//   warps 2-9 epilogue: tile i's accumulator through gemm_epilogue (warp w reads TMEM
+//            lane quadrant w & 3, half of the columns) while tile i + 1 accumulates into
+//            the other one, then release it on its "empty" barrier.
 // TMA writes each box of 8 K-elements x rows as rows x 16 bytes, so a stage of A
 // (128 rows x kKC) is 8 boxes at 2 KB strides: the canonical K-major layout without
 // swizzle with the leading byte offset (next 8 K-elements) 2048 and the stride byte
 // offset (next 8 rows) 128; the weights likewise with N x 16-byte boxes.  Out-of-range
 // rows and K elements are zero-filled by the TMA unit.
+// The epilogue has 8 warps, two per TMEM lane quadrant, each taking half the columns,
+// so that enough TMEM loads are in flight (with 4 warps the epilogue waited on them,
+// long-scoreboard stalls, and held the kernel at ~43 % of DRAM bandwidth).
 // A plain FP32 output (no activation, at most a bias) leaves through TMA stores: each
-// epilogue warp writes its 32 rows x 32 columns into one of two 4 KB staging buffers
-// in the 128-byte swizzled layout (16-byte chunk k of row r at chunk k ^ (r & 7):
+// epilogue warp writes its 32 rows x 32 columns into a 4 KB staging buffer in the
+// 128-byte swizzled layout (16-byte chunk k of row r at chunk k ^ (r & 7):
 // conflict-free) and one lane stores the block with cp.async.bulk.tensor, so HBM sees
-// whole 128-byte rows instead of one 16-byte piece per row per instruction; a buffer
-// is rewritten after the store that read it (bulk wait_group.read).  Every mbarrier
+// whole 128-byte rows instead of one 16-byte piece per row per instruction; the buffer
+// is rewritten after the store has read it (bulk wait_group.read).  Every mbarrier
 // wait is bounded (error word); before freeing TMEM the producer waits (bounded) for
 // its loads in flight, the MMA thread for its last MMAs and the epilogue lanes for
 // their stores.
 constexpr int kWsMaxStages = 4;
-constexpr int kWsThreads = 192;
+constexpr int kWsEpiWarps = 8;
+constexpr int kWsThreads = 32 * (2 + kWsEpiWarps);
 constexpr int kWsStageC = 32 * 32 * 4;  // one epilogue staging buffer (bytes)
 
 __device__ __forceinline__ void mbar_init_n(uint64_t *mbar, uint32_t n) {
@@ -551,7 +556,8 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
 // at least 2.
 inline int gemm_ws_stages(int N, int K, bool tma_store) {
   const int nk = (K + kKC - 1) / kKC;
-  const size_t fixed = (size_t)nk * kKC * N * 2 + (tma_store ? 8 * kWsStageC + 1024 : 0) + 1024;
+  const size_t fixed =
+      (size_t)nk * kKC * N * 2 + (tma_store ? kWsEpiWarps * kWsStageC + 1024 : 0) + 1024;
   const size_t cap = 227 * 1024 - 1024;  // the per-CTA limit less the static barriers
   int st = kWsMaxStages;
   while (st > 2 && fixed + (size_t)st * kTileM * kKC * 2 > cap) --st;
@@ -562,23 +568,24 @@ inline size_t gemm_ws_smem_bytes(int N, int K, bool tma_store) {
   const int nk = (K + kKC - 1) / kKC;
   const size_t need = (size_t)nk * kKC * N * 2 +
                       (size_t)gemm_ws_stages(N, K, tma_store) * kTileM * kKC * 2 +
-                      (tma_store ? 8 * kWsStageC + 1024 : 0);
+                      (tma_store ? kWsEpiWarps * kWsStageC + 1024 : 0);
   return need > (size_t)120 * 1024 ? need : (size_t)120 * 1024;
 }
 
 // Epilogue of one 128-row tile through TMA stores (plain FP32 output, optional bias):
-// warp quadrant `quad`, rows m0 + 32 quad + lane, 32 columns per block.  `cstage`: the
-// warp's two staging buffers (1024-byte aligned); `nst`: stores issued so far by this
-// warp (selects the buffer).
+// warp quadrant `quad`, rows m0 + 32 quad + lane, columns [cbeg, cend) in 32-column
+// blocks.  `cstage`: the warp's staging buffer (1024-byte aligned); `nst`: stores
+// issued so far by this warp.
 __device__ __forceinline__ void gemm_epilogue_tma(const GemmArgs &g, const CUtensorMap *tmC,
-                                                  int m0, uint32_t tmem, int quad,
-                                                  unsigned char *cstage, int &nst) {
+                                                  int m0, uint32_t tmem, int quad, int cbeg,
+                                                  int cend, unsigned char *cstage, int &nst) {
   const int lane = threadIdx.x & 31;
   const int row0 = m0 + quad * 32;
   const uint32_t tq = tmem + ((uint32_t)(quad * 32) << 16);
+  cend = min(cend, g.n_valid);
   // two 32-column blocks per TMEM round trip
-  for (int c0 = 0; c0 < g.n_valid; c0 += 64) {
-    const bool two = c0 + 32 < g.n_valid;
+  for (int c0 = cbeg; c0 < cend; c0 += 64) {
+    const bool two = c0 + 32 < cend;
     uint32_t r[2][32];
     tmem_ld32_async(tq + (uint32_t)c0, r[0]);
     if (two) tmem_ld32_async(tq + (uint32_t)(c0 + 32), r[1]);
@@ -596,9 +603,9 @@ __device__ __forceinline__ void gemm_epilogue_tma(const GemmArgs &g, const CUten
         for (int j = 0; j < 32; ++j)
           if (cb + j < g.n_valid) v[j] += g.bias[cb + j];
       }
-      unsigned char *buf = cstage + (nst & 1) * kWsStageC;
-      if (nst >= 2 && lane == 0)  // the store that read this buffer has read it
-        asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+      unsigned char *buf = cstage;
+      if (nst >= 1 && lane == 0)  // the previous store has read the buffer
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
       __syncwarp();
 #pragma unroll
       for (int k = 0; k < 8; ++k)
@@ -648,7 +655,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init_n(&s_accf[b], 1);
-      mbar_init_n(&s_acce[b], 4);  // one arrival per epilogue warp
+      mbar_init_n(&s_acce[b], kWsEpiWarps);  // one arrival per epilogue warp
     }
     mbar_init_n(&s_bfull, 1);
     mbar_init_n(&s_mdone, 1);
@@ -724,7 +731,11 @@ __global__ void __launch_bounds__(kWsThreads, 1)
     }
   } else {
     const int quad = warp & 3;  // TMEM lane quadrant this warp may read
-    unsigned char *cstage = sC + (size_t)(warp - 2) * 2 * kWsStageC;
+    // the two warps of a quadrant take the first and the second half of the columns
+    const int half = (warp - 2) >> 2;
+    const int ch = (g.N / 2 + 31) / 32 * 32;
+    const int cbeg = half * ch, cend = half ? g.N : ch;
+    unsigned char *cstage = sC + (size_t)(warp - 2) * kWsStageC;
     int nst = 0;  // TMA stores issued by this warp
     for (int i = 0; i < my_tiles; ++i) {
       const int acc = i & 1;
@@ -735,9 +746,10 @@ __global__ void __launch_bounds__(kWsThreads, 1)
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int m0 = (blockIdx.x + i * gridDim.x) * kTileM;
       if (tma_store)
-        gemm_epilogue_tma(g, &tmC, m0, tmem + (uint32_t)acc * nacc, quad, cstage, nst);
+        gemm_epilogue_tma(g, &tmC, m0, tmem + (uint32_t)acc * nacc, quad, cbeg, cend, cstage,
+                          nst);
       else
-        gemm_epilogue(g, m0, tmem + (uint32_t)acc * nacc, g.out, quad);
+        gemm_epilogue(g, m0, tmem + (uint32_t)acc * nacc, g.out, quad, cbeg, cend);
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive1(&s_acce[acc]);

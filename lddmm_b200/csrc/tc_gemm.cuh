@@ -75,6 +75,17 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
+// The same for a K-major operand in the 128-byte swizzled layout (rows of 64 BF16 =
+// 128 bytes at 128-byte strides, 16-byte chunk c of row r stored at chunk c ^ (r & 7),
+// 1024-byte aligned atoms of 8 rows): stride byte offset 1024 (next 8 rows), leading
+// byte offset unused for this layout (16), layout type 2 (128-byte swizzle) in bits
+// 61-63.  A K step of 16 elements inside the 64-element row advances the start address
+// by 32 bytes; the unit applies the swizzle to the addresses it forms.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)(16u >> 4) << 16) |
+         ((uint64_t)(1024u >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+
 // Instruction descriptor, kind::f16: F32 accumulator (bits 4-5 = 1), A and B BF16
 // (7-9 = 1, 10-12 = 1), both K-major (15, 16 = 0), N >> 3 (17-22), M >> 4 (24-28).
 __host__ __device__ constexpr uint32_t instr_desc_bf16(int M, int N) {
@@ -490,11 +501,12 @@ inline size_t gemm_smem_bytes(int N) { return 2 * (size_t)(kTileM + N) * kKC * 2
 //   warps 2-9 epilogue: tile i's accumulator through gemm_epilogue (warp w reads TMEM
 //            lane quadrant w & 3, half of the columns) while tile i + 1 accumulates into
 //            the other one, then release it on its "empty" barrier.
-// TMA writes each box of 8 K-elements x rows as rows x 16 bytes, so a stage of A
-// (128 rows x kKC) is 8 boxes at 2 KB strides: the canonical K-major layout without
-// swizzle with the leading byte offset (next 8 K-elements) 2048 and the stride byte
-// offset (next 8 rows) 128; the weights likewise with N x 16-byte boxes.  Out-of-range
-// rows and K elements are zero-filled by the TMA unit.
+// Operands are loaded as 128-byte swizzled K-major tiles: one TMA box of 64 K-elements
+// (one 128-byte segment of each row) x 128 rows per A stage, one box of 64 x N per
+// 64-element chunk of the weights, so every row segment is a single 128-byte request
+// (boxes 8 elements wide, in the canonical layout without swizzle, cost one 16-byte
+// request per row and held the A stream back).  Out-of-range rows and K elements are
+// zero-filled by the TMA unit.
 // The epilogue has 8 warps, two per TMEM lane quadrant, each taking half the columns,
 // so that enough TMEM loads are in flight (with 4 warps the epilogue waited on them,
 // long-scoreboard stalls, and held the kernel at ~43 % of DRAM bandwidth).
@@ -557,7 +569,7 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, i
 inline int gemm_ws_stages(int N, int K, bool tma_store) {
   const int nk = (K + kKC - 1) / kKC;
   const size_t fixed =
-      (size_t)nk * kKC * N * 2 + (tma_store ? kWsEpiWarps * kWsStageC + 1024 : 0) + 1024;
+      (size_t)nk * kKC * N * 2 + (tma_store ? kWsEpiWarps * kWsStageC : 0) + 2048;
   const size_t cap = 227 * 1024 - 1024;  // the per-CTA limit less the static barriers
   int st = kWsMaxStages;
   while (st > 2 && fixed + (size_t)st * kTileM * kKC * 2 > cap) --st;
@@ -568,7 +580,7 @@ inline size_t gemm_ws_smem_bytes(int N, int K, bool tma_store) {
   const int nk = (K + kKC - 1) / kKC;
   const size_t need = (size_t)nk * kKC * N * 2 +
                       (size_t)gemm_ws_stages(N, K, tma_store) * kTileM * kKC * 2 +
-                      (tma_store ? kWsEpiWarps * kWsStageC + 1024 : 0);
+                      (tma_store ? kWsEpiWarps * kWsStageC : 0) + 1024;  // + alignment
   return need > (size_t)120 * 1024 ? need : (size_t)120 * 1024;
 }
 
@@ -629,15 +641,14 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   __shared__ uint32_t s_tmem;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int nk = (g.K + kKC - 1) / kKC;
-  const uint32_t b_group = (uint32_t)g.N * 16;  // bytes of one 8-element K group of B
+  const uint32_t b_chunk = (uint32_t)g.N * 128;  // bytes of one 64-element K chunk of B
   const int kWsStages = stages;  // A stage buffers (<= kWsMaxStages)
-  unsigned char *sB = smem;
-  unsigned char *sA = smem + (size_t)nk * 8 * b_group;
   constexpr uint32_t kStageBytes = kTileM * kKC * 2;
-  // epilogue staging buffers, 1024-byte aligned (the 128-byte swizzle repeats every
-  // 8 rows of 128 bytes)
-  const uint32_t c_off = (uint32_t)((size_t)nk * 8 * b_group + (size_t)stages * kStageBytes);
-  unsigned char *sC = smem + c_off + ((1024u - ((smem_u32(smem) + c_off) & 1023u)) & 1023u);
+  // every tile 1024-byte aligned (the 128-byte swizzle repeats every 8 rows of 128
+  // bytes): the weights, the A stages, then the epilogue staging buffers
+  unsigned char *sB = smem + ((1024u - (smem_u32(smem) & 1023u)) & 1023u);
+  unsigned char *sA = sB + (size_t)nk * b_chunk;
+  unsigned char *sC = sA + (size_t)stages * kStageBytes;
   const int ntiles = (g.M + kTileM - 1) / kTileM;
   const int my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const uint32_t nacc = g.N <= 32 ? 32u : g.N <= 64 ? 64u : g.N <= 128 ? 128u : 256u;
@@ -671,8 +682,8 @@ __global__ void __launch_bounds__(kWsThreads, 1)
   const int Q = my_tiles * nk;  // (tile, K chunk) steps of this CTA
   if (warp == 0) {
     if (lane == 0) {
-      mbar_expect_tx(&s_bfull, (uint32_t)nk * 8 * b_group);
-      for (int c = 0; c < nk * 8; ++c) tma_load_2d(sB + (size_t)c * b_group, &tmB, c * 8, 0, &s_bfull);
+      mbar_expect_tx(&s_bfull, (uint32_t)nk * b_chunk);
+      for (int c = 0; c < nk; ++c) tma_load_2d(sB + (size_t)c * b_chunk, &tmB, c * kKC, 0, &s_bfull);
       int q = 0;
       for (; q < Q; ++q) {
         const int st = q % kWsStages;
@@ -683,9 +694,7 @@ __global__ void __launch_bounds__(kWsThreads, 1)
         mbar_expect_tx(&s_full[st], kStageBytes);
         const int row = (blockIdx.x + (q / nk) * gridDim.x) * kTileM;
         const int k0 = (q % nk) * kKC;
-        unsigned char *dst = sA + (size_t)st * kStageBytes;
-        for (int c = 0; c < kKC / 8; ++c)
-          tma_load_2d(dst + c * (kTileM * 16), &tmA, k0 + c * 8, row, &s_full[st]);
+        tma_load_2d(sA + (size_t)st * kStageBytes, &tmA, k0, row, &s_full[st]);
       }
       // the loads in flight complete before the CTA leaves (bounded)
       for (int r = (q > kWsStages ? q - kWsStages : 0); r < q; ++r)
@@ -714,11 +723,11 @@ __global__ void __launch_bounds__(kWsThreads, 1)
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t a0 = smem_u32(sA + (size_t)st * kStageBytes);
-          const uint32_t b0 = smem_u32(sB + (size_t)kc * 8 * b_group);
+          const uint32_t b0 = smem_u32(sB + (size_t)kc * b_chunk);
 #pragma unroll
           for (int s = 0; s < kKC / 16; ++s) {
-            const uint64_t da = smem_desc(a0 + s * 2 * (kTileM * 16), kTileM * 16, 128);
-            const uint64_t db = smem_desc(b0 + s * 2 * b_group, b_group, 128);
+            const uint64_t da = smem_desc_sw128(a0 + s * 32);
+            const uint64_t db = smem_desc_sw128(b0 + s * 32);
             mma_bf16(d, da, db, idesc, (kc == 0 && s == 0) ? 0u : 1u);
           }
           mma_commit(&s_empty[st]);

@@ -362,18 +362,19 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 // 2D TMA map of a K-major BF16 matrix (rows x K, row stride ld elements) read in boxes
-// of 8 K-elements x box_rows rows; false when the operand does not meet TMA's rules
-// (16-byte aligned base and row stride) or the encoder refuses it.
+// of 64 K-elements (128 bytes) x box_rows rows into the 128-byte swizzled layout;
+// false when the operand does not meet TMA's rules (16-byte aligned base and row
+// stride) or the encoder refuses it.
 bool make_kmajor_map(CUtensorMap *m, const void *base, long long K, long long rows,
                      long long ld, int box_rows) {
   const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
   if (!enc || ((uintptr_t)base & 15u) || (ld * 2) % 16 || K < 8 || rows < 1) return false;
   cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
   cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-  cuuint32_t box[2] = {8u, (cuuint32_t)box_rows};
+  cuuint32_t box[2] = {(cuuint32_t)kKC, (cuuint32_t)box_rows};
   cuuint32_t es[2] = {1u, 1u};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides,
-             box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
          CUDA_SUCCESS;
 }

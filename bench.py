@@ -268,11 +268,16 @@ def population_leg(stream, local, flush):
                 e1.record(stream)
                 torch.cuda.synchronize()
                 ms.append(e0.elapsed_time(e1))
-            return statistics.median(ms), [dict(iters=r.iters, evals=r.evals, status=r.status,
-                                                f=r.fcn) for r in res], ctx.counters()
+            out = [dict(iters=r.iters, evals=r.evals, status=r.status, f=r.fcn) for r in res]
+            cnt = ctx.counters()
+            # after the timed runs: one evaluation's sweeps and the tuned launch shape
+            info = {"sweep_ms": {k: round(float(v), 4) for k, v in
+                                 ctx.time_sweeps(reps=1).items()},
+                    "launch_shape": ctx.launch_shape()}
+            return statistics.median(ms), out, cnt, info
 
     with ClockSampler(local) as clk:
-        ms_all, res_all, cnt = batch(probs, 2)
+        ms_all, res_all, cnt, info = batch(probs, 2)
     clocks = clk.summary()
     pairs_eval = [2 * P.T * P.nde_num ** 2 + P.dfm_elm_num * (P.dfm_elm_num + P.tgt_elm_num)
                   for P in probs]
@@ -299,7 +304,7 @@ def population_leg(stream, local, flush):
     ref_lbfgs_s = sum(r["ms_lbfgs"] for r in ref) * 1e-3
     ref_total_s = sum(r["ms_total"] for r in ref) * 1e-3
     est_lbfgs_s = sum(len(st) * r["ms_lbfgs"] for st, r in zip(strata, ref)) * 1e-3
-    ms_sample, _, _ = batch([probs[k] for k in pick], 2)
+    ms_sample, _, _, _ = batch([probs[k] for k in pick], 2)
     secs = ms_all * 1e-3
     return {
         "workload": POP_WORKLOAD, "pairs": POP_PAIRS,
@@ -309,6 +314,7 @@ def population_leg(stream, local, flush):
         "iters_max": int(max(r["iters"] for r in res_all)),
         "status": sorted({int(r["status"]) for r in res_all}),
         "kernel_launches": cnt["launches"], "generation_s": t_gen, "clocks": clocks,
+        "cycle": info,
         "fp64_gpu_reference": {
             "path": "reference CUDA/src (FP64, cuBLAS), compiled unmodified for sm_100a",
             "sample": f"{POP_SAMPLE} pairs, one per stratum of the pairs sorted by work "

@@ -89,6 +89,20 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
   return v;
 }
 
+// Arrival count with release semantics (orders this thread's writes, and those of
+// threads synchronised with it, before the increment) and no return value.
+__device__ __forceinline__ void red_add_release_gpu(unsigned int *p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Atomic add at GPU scope with release and acquire semantics; returns the old value.
+__device__ __forceinline__ unsigned int atom_add_acq_rel_gpu(unsigned int *p, unsigned int v) {
+  unsigned int old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v)
+               : "memory");
+  return old;
+}
+
 __device__ __forceinline__ unsigned int ld_relaxed(const unsigned int *p) {
   unsigned int v;
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -97,9 +111,10 @@ __device__ __forceinline__ unsigned int ld_relaxed(const unsigned int *p) {
 
 // Waits until `target` arrivals (this CTA's included) have been counted.  Returns
 // false when the wait timed out (the caller must leave the kernel without departing).
-// `tag` identifies the wait in the error word.  The poll is one relaxed load per
-// iteration (the error word is read every 64th); the fence after the loop orders the
-// CTA's later reads after the arrivals it observed.
+// `tag` identifies the wait in the error word.  The arrival is a release reduction
+// (the CTA's writes, ordered before it by __syncthreads, become visible with it); the
+// poll is one relaxed load per iteration (the error word is read every 64th); the
+// fence after the loop orders the CTA's later reads after the arrivals it observed.
 __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
                                              unsigned int tag,
                                              unsigned int spin = kSpinLimit) {
@@ -107,8 +122,7 @@ __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    fence_acq_rel_gpu();
-    atomicAdd(&sy->arrive, 1u);
+    red_add_release_gpu(&sy->arrive, 1u);
     unsigned int n = 0;
     while (ld_relaxed(&sy->arrive) < target) {
       if ((++n & 63u) == 0u) {
@@ -336,15 +350,13 @@ __global__ void __launch_bounds__(kPersistWarps * 32, 2)
           double *slot = plan.part + ((size_t)(up.y + se.w) * kGroup + lane) * kPartNA;
 #pragma unroll
           for (int a = 0; a < NA; ++a) slot[a] = v[a];
-          fence_acq_rel_gpu();
-          __syncwarp(0xffffu);
+          __syncwarp(0xffffu);  // the 16 lanes' part writes before lane 0's release
           int last = 0;
           if (lane == 0) {
-            last = atomicAdd(&plan.cnt[se.x], 1u) == (unsigned int)up.x - 1u;
-            if (last) {
-              plan.cnt[se.x] = 0u;  // next step's arrivals come after the grid barrier
-              fence_acq_rel_gpu();
-            }
+            // release: this part is visible with the count; acquire: the last arriver
+            // sees every other part
+            last = atom_add_acq_rel_gpu(&plan.cnt[se.x], 1u) == (unsigned int)up.x - 1u;
+            if (last) plan.cnt[se.x] = 0u;  // next step's arrivals come after the barrier
           }
           fin = __shfl_sync(0xffffu, last, 0) != 0;
           __syncwarp(0xffffu);

@@ -76,13 +76,6 @@ __device__ __forceinline__ void stamp_exit(StepSync *sy, int slot) {
 
 constexpr unsigned int kSpinLimit = 1u << 23;  // polls: a few seconds at most
 
-// Release / acquire fence at GPU scope: orders this thread's (and, cumulatively, its
-// CTA's synchronised) writes before a later relaxed atomic, and an observed atomic
-// before later reads.  Lighter than the sequentially consistent __threadfence().
-__device__ __forceinline__ void fence_acq_rel_gpu() {
-  asm volatile("fence.acq_rel.gpu;" ::: "memory");
-}
-
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int *p) {
   unsigned int v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -113,8 +106,8 @@ __device__ __forceinline__ unsigned int ld_relaxed(const unsigned int *p) {
 // false when the wait timed out (the caller must leave the kernel without departing).
 // `tag` identifies the wait in the error word.  The arrival is a release reduction
 // (the CTA's writes, ordered before it by __syncthreads, become visible with it); the
-// poll is one relaxed load per iteration (the error word is read every 64th); the
-// fence after the loop orders the CTA's later reads after the arrivals it observed.
+// poll is one relaxed load per iteration (the error word is read every 64th); one
+// acquire load after the loop orders the CTA's later reads after the arrivals.
 __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
                                              unsigned int tag,
                                              unsigned int spin = kSpinLimit) {
@@ -134,7 +127,9 @@ __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
         if (n > 4096u) __nanosleep(64);
       }
     }
-    fence_acq_rel_gpu();
+    // acquire: the count read here is the end of the release sequence of every CTA's
+    // arrival (each arrival is a read-modify-write), so their writes are visible
+    if (ok) (void)ld_acquire(&sy->arrive);
     s_ok = ok;
   }
   __syncthreads();

@@ -111,6 +111,24 @@ def sphere2cube_example_columns():
          opt=np.array([40, 1e-2, 0.0, 0.5, 10000]))
 
 
+def sphere2cube_example_full():
+    """The reference's example exactly as run_sphere2cube.m:27-31 calls it
+    (MaxIterations 100000, OptimalityTolerance 1e-2, Wolfe 0 / 0.5, Columns 10000), run
+    until its own stopping test; the final landmarks are the returned momenta shot by the
+    FP64 oracle (computeNodePosition)."""
+    from oracle.oracle import Oracle
+
+    P = _sphere2cube_example_problem()
+    R = Reference(3)
+    r = R.lbfgs(P, np.zeros(P.var_num), itr_max=100000, tol=1e-2, wolfe1=0.0, wolfe2=0.5,
+                mem_num=10000)
+    nde, _ = Oracle().shoot(P.ini_nde, r["x"], P.knl_order, P.knl_width, P.time_stp,
+                            P.time_num)
+    save("sphere2cube_example_full", f=np.array(r["f"]), ret=np.array(r["ret"]),
+         evals=np.array(r["evals"]), nde_final=nde[-1], trace_f=r["trace_f"],
+         opt=np.array([100000, 1e-2, 0.0, 0.5, 10000]))
+
+
 def sphere2cube_example():
     P = _sphere2cube_example_problem()
     R = Reference(3)
@@ -223,6 +241,7 @@ ALL = {
     "circle2square_example": circle2square_example,
     "sphere2cube_example": sphere2cube_example,
     "sphere2cube_example_columns": sphere2cube_example_columns,
+    "sphere2cube_example_full": sphere2cube_example_full,
     "varifold_types": varifold_types,
     "objgrd_orders_3d": objgrd_orders_3d,
     "objgrd_orders_2d": objgrd_orders_2d,

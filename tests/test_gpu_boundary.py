@@ -136,3 +136,30 @@ def test_memory_beyond_the_device_is_refused_cleanly():
         # the context stays usable
         x, r = ctx.lbfgs(np.zeros(ctx.var_total), itr_max=2, mem_num=5)
         assert r[0]["iters"] == 2
+
+
+def test_LDDMM_runs_the_reference_example_to_its_end():
+    """The reference's example exactly as it calls the MEX (MaxIterations 100000,
+    OptimalityTolerance 1e-2, Wolfe 0 / 0.5, Columns 10000), through lddmm_LDDMM,
+    run until the |g| test stops it (the reference: 139 evaluations; here ~101
+    iterations): the returned momenta's objective within 1e-5 relative of the
+    reference's final objective and the deformed landmarks within 1e-4 of the shape
+    diameter of the reference's (tests/golden/make_golden.py
+    sphere2cube_example_full)."""
+    from lddmm_b200 import api
+
+    z = golden("sphere2cube_example")
+    zf = golden("sphere2cube_example_full")
+    P = problem_from(z)
+    itr, tol, w1, w2, cols = zf["opt"]
+    rc, x = _call_LDDMM(P, itr, tol, w1, w2, cols, verbose=False)
+    assert rc == int(zf["ret"]) == 0
+    with api.Context(P) as ctx:
+        f, _ = ctx.objgrd(x)
+        (nde, _), = ctx.shoot(x)
+    rel_f = abs(f[0] - float(zf["f"])) / abs(float(zf["f"]))
+    err = np.sqrt(np.mean(np.sum((nde[-1] - zf["nde_final"]) ** 2, axis=1))) / P.diameter()
+    print(f"f {f[0]:.9g} vs reference {float(zf['f']):.9g} (rel {rel_f:.1e}); landmarks "
+          f"RMS {err:.1e} of the diameter")
+    assert rel_f < 1e-5, rel_f
+    assert err < 1e-4, err

@@ -264,10 +264,12 @@ def evaluate(ws: WarmStart, seeds, batch=64, itr_max=300, rel_obj_tol=1e-6, rel=
 
 
 def experiment(n_train=4096, n_test=512, subdiv=4, epochs=400, batch=64, lr=1e-3, seed=0,
-               log=print):
+               log=print, eval_itr_max=1000, eval_rel_obj_tol=1e-9):
     """The learned-warm-start workload end to end: plain-method registrations of
     n_train + n_test pairs (training seeds 1000.., held-out seeds 50000..), training,
-    then cold vs warm start on the held-out pairs.  Returns a JSON-ready dict."""
+    then cold vs warm start on the held-out pairs, both run to convergence (relative
+    objective change below eval_rel_obj_tol, at most eval_itr_max iterations).
+    Returns a JSON-ready dict."""
     import functools
 
     import torch
@@ -285,7 +287,8 @@ def experiment(n_train=4096, n_test=512, subdiv=4, epochs=400, batch=64, lr=1e-3
         hist = train(ws, tri, lab, epochs=epochs, batch=batch, lr=lr, seed=seed)
         torch.cuda.synchronize()
         t_train = time.perf_counter() - t0
-        ev = evaluate(ws, list(range(50000, 50000 + n_test)), batch=batch, make=make)
+        ev = evaluate(ws, list(range(50000, 50000 + n_test)), batch=batch, make=make,
+                      itr_max=eval_itr_max, rel_obj_tol=eval_rel_obj_tol)
     rows = ev.pop("rows")
     ratio = [r["f_start_warm"] / r["f_start_cold"] for r in rows]
     return dict(n_train=n_train, n_test=n_test, landmarks=int(src.shape[0]),

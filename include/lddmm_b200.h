@@ -351,9 +351,20 @@ int lddmm_ws_grad(lddmm_ws *ws, const float *d_tri7, int pairs, int tri_num,
 int lddmm_ws_train_step(lddmm_ws *ws, const float *d_tri7, int pairs, int tri_num,
                         const float *d_labels, double lr, double *loss);
 /* Predicted momenta of `pairs` pairs in the variable layout (pairs x T x n_src x 3,
- * FP64), ready as the initial point of lddmm_lbfgs_device. */
+ * FP64), ready as the initial point of lddmm_lbfgs_device.  The activations stay on
+ * the context for lddmm_ws_backward until the weights change. */
 int lddmm_ws_predict(lddmm_ws *ws, const float *d_tri7, int pairs, int tri_num,
                      double *d_alpha);
+/* Backward pass of the last lddmm_ws_predict's batch for the loss
+ *   label_weight * MSE(labels)  +  sum d_dalpha . alpha
+ * d_labels as in lddmm_ws_grad (NULL: no MSE term); d_dalpha: the gradient of an outer
+ * loss with respect to the predicted momenta, in their variable layout (pairs x T x
+ * n_src x 3 FP64, e.g. lddmm_objgrd_device's gradient at the prediction, scaled), or
+ * NULL.  lr > 0: one Adam step (the activations are then spent); lr = 0: the gradient
+ * only.  grad_host (num_params floats) and loss (the MSE term, 0 without labels) may be
+ * NULL.  LDDMM_ERR_ARG without a prediction since the last weight change. */
+int lddmm_ws_backward(lddmm_ws *ws, const float *d_labels, double label_weight,
+                      const double *d_dalpha, double lr, float *grad_host, double *loss);
 /* The network's BF16 tensor-core GEMM on its own: C[m x n] (FP32, leading dimension
  * ldc) = A[m x k] . B[n x k]^T, A and B BF16 row-major with k contiguous; n = 16..256
  * in steps of 16, k a multiple of 16, lda and ldb multiples of 8.  Asynchronous on

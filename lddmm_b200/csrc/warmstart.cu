@@ -149,11 +149,14 @@ __global__ void point_input_kernel(const float *xyz, int N, int Np, int B, const
   }
 }
 
-// dy = 2 (y - label / scale) / count on real rows / columns, 0 elsewhere; block
-// partials of the squared error
+// dy = label_weight 2 (y - label / scale) / count (when label is given) + scale *
+// dalpha[p][(t N + i) 3 + d] at column c = 3 t + d (when dalpha is given: the gradient
+// of an outer loss with respect to the predicted momenta, alpha = scale y) on real rows /
+// columns, 0 elsewhere; block partials of the squared error
 __global__ void loss_kernel(const float *y, int ldy, const float *label, float inv_scale, int N,
                             int Np, int B, int n_out, int n_out_pad, float inv_count, bf16 *dy,
-                            bf16 *dyT, double *part) {
+                            bf16 *dyT, double *part, float label_weight = 1.0f,
+                            const double *dalpha = nullptr, float scale = 1.0f, int T = 0) {
   __shared__ double s[kThreads / 32];
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long M = (long long)B * Np;
@@ -164,10 +167,16 @@ __global__ void loss_kernel(const float *y, int ldy, const float *label, float i
     const int p = (int)(r / Np), i = (int)(r - (long long)p * Np);
     float d = 0.0f;
     if (i < N && c < n_out) {
-      const float t = label[((size_t)p * N + i) * n_out + c] * inv_scale;
-      const float e = y[r * ldy + c] - t;
-      sq = (double)e * e;
-      d = 2.0f * e * inv_count;
+      if (label) {
+        const float t = label[((size_t)p * N + i) * n_out + c] * inv_scale;
+        const float e = y[r * ldy + c] - t;
+        sq = (double)e * e;
+        d = 2.0f * e * inv_count * label_weight;
+      }
+      if (dalpha) {
+        const int t = c / 3, dd = c - 3 * (c / 3);
+        d += scale * (float)dalpha[(size_t)p * T * N * 3 + ((size_t)t * N + i) * 3 + dd];
+      }
     }
     const bf16 h = __float2bfloat16_rn(d);
     dy[r * n_out_pad + c] = h;
@@ -284,6 +293,7 @@ __global__ void predict_out_kernel(const float *y, int ldy, int N, int Np, int B
 struct lddmm_ws {
   int N = 0, Np = 0, T = 0, n_out = 0, n_out_pad = 0, batch_max = 0, et_max = 0, etp_max = 0;
   float label_scale = 1.0f;
+  int fwd_pairs = 0, fwd_tris = 0;  // batch of the activations of the last prediction
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   Layer L[5];  // T1, T2, P1, P2, P3
@@ -552,11 +562,11 @@ int forward(lddmm_ws &w, const float *tri7, int B, int Et) {
   return 0;
 }
 
-// forward + loss + backward: gradient in w.grad, loss (mean squared error) in *loss
-int forward_backward(lddmm_ws &w, const float *tri7, int B, int Et, const float *labels,
-                     double *loss) {
-  int rc = forward(w, tri7, B, Et);
-  if (rc) return rc;
+// output gradient (labels and / or dalpha, loss_kernel) + backward of the activations
+// the last forward left: gradient in w.grad, loss (mean squared error, 0 without labels)
+// in *loss
+int backward(lddmm_ws &w, int B, int Et, const float *labels, float label_weight,
+             const double *dalpha, double *loss) {
   const int Etp = round16(Et);
   const long long Mt = (long long)B * Etp, Mp = (long long)B * w.Np;
   const long long nl = Mp * w.n_out_pad;
@@ -568,7 +578,8 @@ int forward_backward(lddmm_ws &w, const float *tri7, int B, int Et, const float 
   const float inv_count = 1.0f / (float)((double)B * w.N * w.n_out);
   loss_kernel<<<nb, kThreads, 0, w.stream>>>(w.y, w.n_out_pad, labels, 1.0f / w.label_scale, w.N,
                                              w.Np, B, w.n_out, w.n_out_pad, inv_count, w.dy,
-                                             w.dyT, w.loss_part);
+                                             w.dyT, w.loss_part, label_weight, dalpha,
+                                             w.label_scale, w.T);
   // P3: weight gradient, then input gradient through gelu'(pre_a2)
   WCU(weight_grad(w, w.L[4], w.dyT, w.a2T, Mp));
   GemmArgs a = {};
@@ -638,6 +649,22 @@ int forward_backward(lddmm_ws &w, const float *tri7, int B, int Et, const float 
   for (double x : hp) s += x;
   if (loss) *loss = s / ((double)B * w.N * w.n_out);
   return 0;
+}
+
+// forward + loss + backward: gradient in w.grad, loss (mean squared error) in *loss
+int forward_backward(lddmm_ws &w, const float *tri7, int B, int Et, const float *labels,
+                     double *loss) {
+  int rc = forward(w, tri7, B, Et);
+  if (rc) return rc;
+  return backward(w, B, Et, labels, 1.0f, nullptr, loss);
+}
+
+void adam_step(lddmm_ws &w, double lr) {
+  ++w.step;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.0f - std::pow(b1, (float)w.step), c2 = 1.0f - std::pow(b2, (float)w.step);
+  adam_kernel<<<(unsigned)((w.n_params + kThreads - 1) / kThreads), kThreads, 0, w.stream>>>(
+      w.params, w.grad, w.m, w.v, w.n_params, (float)lr, b1, b2, 1e-8f, c1, c2);
 }
 
 }  // namespace
@@ -763,6 +790,7 @@ extern "C" int lddmm_ws_params(lddmm_ws *w, float *host, int set) {
     return LDDMM_ERR_ARG;
   }
   if (set) {
+    w->fwd_pairs = 0;
     WCU(cudaMemcpyAsync(w->params, host, sizeof(float) * w->n_params, cudaMemcpyHostToDevice,
                         w->stream));
     WCU(refresh_bf16(*w));
@@ -782,6 +810,7 @@ extern "C" int lddmm_ws_grad(lddmm_ws *w, const float *d_tri7, int pairs, int tr
   }
   int rc = check_batch(*w, pairs, tri_num);
   if (rc) return rc;
+  w->fwd_pairs = 0;
   rc = forward_backward(*w, d_tri7, pairs, tri_num, d_labels, loss);
   if (rc) return rc;
   if (grad_host) {
@@ -800,15 +829,40 @@ extern "C" int lddmm_ws_train_step(lddmm_ws *w, const float *d_tri7, int pairs, 
   }
   int rc = check_batch(*w, pairs, tri_num);
   if (rc) return rc;
+  w->fwd_pairs = 0;
   rc = forward_backward(*w, d_tri7, pairs, tri_num, d_labels, loss);
   if (rc) return rc;
-  ++w->step;
-  const float b1 = 0.9f, b2 = 0.999f;
-  const float c1 = 1.0f - std::pow(b1, (float)w->step), c2 = 1.0f - std::pow(b2, (float)w->step);
-  adam_kernel<<<(unsigned)((w->n_params + kThreads - 1) / kThreads), kThreads, 0, w->stream>>>(
-      w->params, w->grad, w->m, w->v, w->n_params, (float)lr, b1, b2, 1e-8f, c1, c2);
+  adam_step(*w, lr);
   WCU(cudaGetLastError());
   WCU(refresh_bf16(*w));
+  return 0;
+}
+
+extern "C" int lddmm_ws_backward(lddmm_ws *w, const float *d_labels, double label_weight,
+                                 const double *d_dalpha, double lr, float *grad_host,
+                                 double *loss) {
+  if (!w || !(lr >= 0) || (!d_labels && !d_dalpha) || (d_labels && !(label_weight >= 0))) {
+    ws_err("lddmm_ws_backward: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  if (w->fwd_pairs < 1) {
+    ws_err("lddmm_ws_backward: no lddmm_ws_predict since the last weight change");
+    return LDDMM_ERR_ARG;
+  }
+  const int B = w->fwd_pairs, Et = w->fwd_tris;
+  int rc = backward(*w, B, Et, d_labels, (float)label_weight, d_dalpha, loss);
+  if (rc) return rc;
+  if (grad_host) {
+    WCU(cudaMemcpyAsync(grad_host, w->grad, sizeof(float) * w->n_params, cudaMemcpyDeviceToHost,
+                        w->stream));
+    WCU(cudaStreamSynchronize(w->stream));
+  }
+  if (lr > 0) {
+    w->fwd_pairs = 0;
+    adam_step(*w, lr);
+    WCU(cudaGetLastError());
+    WCU(refresh_bf16(*w));
+  }
   return 0;
 }
 
@@ -820,8 +874,11 @@ extern "C" int lddmm_ws_predict(lddmm_ws *w, const float *d_tri7, int pairs, int
   }
   int rc = check_batch(*w, pairs, tri_num);
   if (rc) return rc;
+  w->fwd_pairs = 0;
   rc = forward(*w, d_tri7, pairs, tri_num);
   if (rc) return rc;
+  w->fwd_pairs = pairs;
+  w->fwd_tris = tri_num;
   const long long n = (long long)pairs * w->T * w->N * 3;
   predict_out_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, w->stream>>>(
       w->y, w->n_out_pad, w->N, w->Np, pairs, w->T, (double)w->label_scale, d_alpha);

@@ -171,6 +171,19 @@ class WarmStart:
                                          C.byref(loss)))
         return loss.value
 
+    def backward(self, labels=None, label_weight=1.0, dalpha=None, lr=0.0, want_grad=False):
+        """Backward pass of the last predict()'s batch for the loss
+        label_weight * MSE(labels) + sum(dalpha * alpha) (dalpha: (pairs, T * N * 3)
+        float64 on the device, the outer loss's gradient at the prediction); one Adam step
+        when lr > 0.  Returns (the MSE term, the gradient when want_grad else None)."""
+        g = np.zeros(self.n_params, dtype=np.float32) if want_grad else None
+        loss = C.c_double()
+        check_ws(lib.lddmm_ws_backward(
+            self._h, C.c_void_p(labels.data_ptr()) if labels is not None else None,
+            label_weight, C.c_void_p(dalpha.data_ptr()) if dalpha is not None else None, lr,
+            g.ctypes.data_as(C.POINTER(C.c_float)) if g is not None else None, C.byref(loss)))
+        return loss.value, g
+
     def predict(self, tri7):
         """Predicted momenta, (pairs, T * N * 3) float64 on the device."""
         import torch
@@ -202,6 +215,66 @@ def train(ws: WarmStart, tri7, labels, epochs=20, batch=64, lr=1e-3, seed=0, log
         if log:
             log(f"epoch {ep + 1}/{epochs}: loss {hist[-1]:.4e}")
     return hist
+
+
+def train_objective(ws: WarmStart, probs, tri7, labels=None, epochs=50, batch=64, lr=3e-4,
+                    label_weight=0.0, seed=0, log=None):
+    """Amortised training on the registration objective itself.  The pairs are cut
+    into fixed batches of `batch`, one batched context each; every step predicts a
+    batch's momenta, evaluates the plain method's objective and gradient there
+    (lddmm_objgrd_device) and back-propagates
+
+        sum_p f_p(alpha_p) / (B f_p(0))  (+ label_weight * MSE(labels)),
+
+    f_p(0) the objective at zero momenta, so every pair weighs the same.  The loss is
+    the quantity a warm start should make small, in the metric of the objective (the
+    kernel-weighted energy and the matching term), where the label loss weighs every
+    momentum component alike.  Batches are visited in a shuffled order each epoch.
+    Returns the mean normalised objective of every epoch."""
+    import torch
+
+    nb = len(probs) // batch
+    ctxs, f0s = [], []
+    try:
+        for b in range(nb):
+            ctx = api.Context(probs[b * batch:(b + 1) * batch])
+            ctxs.append(ctx)
+            z = torch.zeros(ctx.var_total, dtype=torch.float64, device="cuda")
+            f = torch.empty(batch, dtype=torch.float64, device="cuda")
+            g = torch.empty_like(z)
+            torch.cuda.synchronize()
+            check(lib.lddmm_objgrd_device(ctx.handle, C.c_void_p(z.data_ptr()),
+                                          C.c_void_p(f.data_ptr()), C.c_void_p(g.data_ptr()), 0))
+            f0s.append(f.clone())
+        gen = torch.Generator(device="cpu").manual_seed(seed)
+        hist = []
+        for ep in range(epochs):
+            tot, cnt = 0.0, 0
+            for b in torch.randperm(nb, generator=gen).tolist():
+                sl = slice(b * batch, (b + 1) * batch)
+                tri = tri7[sl].contiguous()
+                a = ws.predict(tri)
+                f = torch.empty(batch, dtype=torch.float64, device="cuda")
+                g = torch.empty_like(a)
+                check(lib.lddmm_objgrd_device(ctxs[b].handle, C.c_void_p(a.data_ptr()),
+                                              C.c_void_p(f.data_ptr()),
+                                              C.c_void_p(g.data_ptr()), 0))
+                rel_f = f / f0s[b]
+                if not bool(torch.isfinite(rel_f).all()):
+                    continue
+                dalpha = (g / (f0s[b] * batch)[:, None]).contiguous()
+                torch.cuda.synchronize()
+                lab = labels[sl].contiguous() if (labels is not None and label_weight > 0) else None
+                ws.backward(labels=lab, label_weight=label_weight, dalpha=dalpha, lr=lr)
+                tot += float(rel_f.mean())
+                cnt += 1
+            hist.append(tot / max(cnt, 1))
+            if log:
+                log(f"objective epoch {ep + 1}/{epochs}: mean f / f(0) {hist[-1]:.5e}")
+        return hist
+    finally:
+        for ctx in ctxs:
+            ctx.close()
 
 
 def _time_to(trace, f_target):

@@ -57,10 +57,14 @@ def gelu_grad(x):
     return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2.0 * np.pi)
 
 
-def loss_and_grad(params, xyz, tri7, labels, T, label_scale, bf=True):
-    """Mean squared error of a batch and its gradient (flat, the library's layout).
+def loss_and_grad(params, xyz, tri7, labels, T, label_scale, bf=True, label_weight=1.0,
+                  dalpha=None):
+    """Mean squared error of a batch and the gradient (flat, the library's layout) of
+    label_weight * MSE + sum(dalpha * alpha), alpha = label_scale * y the predicted
+    momenta.
 
-    xyz (N, 3) source landmarks; tri7 (B, Et, 7) target features; labels (B, N, 3T)."""
+    xyz (N, 3) source landmarks; tri7 (B, Et, 7) target features; labels (B, N, 3T) or
+    None (no MSE term); dalpha (B, T, N, 3) or None."""
     r = to_bf16 if bf else (lambda v: np.asarray(v, dtype=np.float64))
     params = np.asarray(params, dtype=np.float64)
     L = unpack(params, T)
@@ -88,10 +92,15 @@ def loss_and_grad(params, xyz, tri7, labels, T, label_scale, bf=True):
     a2 = r(gelu(pre2))
     y = a2 @ r(P3).T + c3
     count = B * N * n_out
-    e = y[:, :, :n_out] - labels / label_scale
-    loss = float(np.sum(e * e) / count)
     dy = np.zeros_like(y)
-    dy[:, :, :n_out] = 2.0 * e / count
+    loss = 0.0
+    if labels is not None:
+        e = y[:, :, :n_out] - labels / label_scale
+        loss = float(np.sum(e * e) / count)
+        dy[:, :, :n_out] = label_weight * 2.0 * e / count
+    if dalpha is not None:
+        dy[:, :, :n_out] += label_scale * np.asarray(dalpha).transpose(0, 2, 1, 3).reshape(
+            B, N, n_out)
     dy = r(dy)
     grads = []
     dP3 = np.einsum("bno,bni->oi", dy, a2)

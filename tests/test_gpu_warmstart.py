@@ -75,6 +75,34 @@ def test_loss_and_gradient_vs_oracle(ws_mod):
     assert np.linalg.norm(g - go) / np.linalg.norm(go) < 5e-3
 
 
+def test_backward_with_an_outer_gradient_vs_oracle(ws_mod):
+    """lddmm_ws_backward after a prediction: the gradient of label_weight * MSE + the
+    outer loss sum(dalpha * alpha) against the oracle, with and without labels; the
+    weights stay as they are with lr = 0."""
+    T, scale = 3, 0.05
+    B, N = 3, 50
+    xyz, tri7, labels = _case(T)
+    params = M.init_params(T, seed=6).astype(np.float32)
+    dalpha = np.random.default_rng(3).normal(size=(B, T, N, 3)) * 1e-3
+    t = torch.from_numpy(tri7.astype(np.float32)).cuda()
+    y = torch.from_numpy(labels.astype(np.float32)).cuda()
+    d = torch.from_numpy(dalpha.reshape(B, -1)).cuda()
+    args = (params.astype(np.float64), xyz.astype(np.float32).astype(np.float64),
+            tri7.astype(np.float32).astype(np.float64))
+    with ws_mod.WarmStart(xyz, T, batch_max=4, tri_max=64, label_scale=scale) as ws:
+        ws.params = params
+        ws.predict(t)
+        loss, g = ws.backward(labels=y, label_weight=0.5, dalpha=d, want_grad=True)
+        lo, go = M.loss_and_grad(*args, labels.astype(np.float32).astype(np.float64), T, scale,
+                                 bf=True, label_weight=0.5, dalpha=dalpha)
+        assert abs(loss - lo) <= 1e-4 * abs(lo)
+        assert np.linalg.norm(g - go) / np.linalg.norm(go) < 5e-3
+        _, g2 = ws.backward(dalpha=d, want_grad=True)
+        _, go2 = M.loss_and_grad(*args, None, T, scale, bf=True, dalpha=dalpha)
+        assert np.linalg.norm(g2 - go2) / np.linalg.norm(go2) < 5e-3
+        assert np.array_equal(ws.params, params)
+
+
 def test_predict_vs_oracle(ws_mod):
     T, scale = 3, 0.05
     xyz, tri7, _ = _case(T, seed=1)

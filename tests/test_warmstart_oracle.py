@@ -57,3 +57,27 @@ def test_padding_gradients_are_zero():
         off += o * i
         assert np.all(g[off + orr:off + o] == 0)
         off += o
+
+
+def test_outer_gradient_term_finite_differences():
+    """The gradient of sum(dalpha * alpha(params)) (an outer loss's gradient at the
+    prediction, back-propagated through the network) against central differences of
+    the oracle's own prediction."""
+    T, scale = 2, 0.7
+    params, xyz, tri7, _ = _case(T, seed=4)
+    B, N = tri7.shape[0], xyz.shape[0]
+    dalpha = np.random.default_rng(5).normal(size=(B, T, N, 3))
+    _, g = M.loss_and_grad(params, xyz, tri7, None, T, scale, bf=False, dalpha=dalpha)
+
+    def outer(p):
+        a = M.predict(p, xyz, tri7, T, scale, bf=False)
+        return float(np.sum(a.reshape(dalpha.shape) * dalpha))
+
+    rng = np.random.default_rng(6)
+    h = 1e-6
+    for k in rng.choice(np.flatnonzero(g != 0), 24, replace=False):
+        p1, p2 = params.copy(), params.copy()
+        p1[k] += h
+        p2[k] -= h
+        fd = (outer(p1) - outer(p2)) / (2 * h)
+        assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(g[k])) + 1e-8, (k, fd, g[k])

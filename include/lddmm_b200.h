@@ -170,6 +170,14 @@ int lddmm_objgrd(lddmm_ctx *ctx, const double *alp, double *fcn, double *grd);
 int lddmm_objgrd_device(lddmm_ctx *ctx, const double *d_alp, double *d_fcn, double *d_grd,
                         int async);
 
+/* objgrd on device buffers (synchronous) that also returns the adjoint costate:
+ * d_pst (like alp) receives, for every step t, p_{t+1}, the costate the backward
+ * recursion multiplies at step t -- the gradient of step t is dt K(q_t) (alpha_t -
+ * p_{t+1}) (objgrd.cpp:67-87), so alpha_t = p_{t+1} at a stationary point.  d_grd may
+ * be NULL. */
+int lddmm_objgrd_costate(lddmm_ctx *ctx, const double *d_alp, double *d_fcn, double *d_grd,
+                         double *d_pst);
+
 /* L-BFGS from alp_inout (host) for every pair; on return alp_inout holds each pair's
  * last accepted point (the reference's posNow) and res[num] the outcome.  Returns 0
  * when every pair ended with status 0, else the first nonzero status. */

@@ -19,7 +19,7 @@ _ip = C.POINTER(C.c_int)
 EXPORTS = [
     "lddmm_last_error", "lddmm_version", "lddmm_ctx_create", "lddmm_ctx_destroy",
     "lddmm_ctx_num_pairs", "lddmm_ctx_var_num", "lddmm_ctx_var_offset", "lddmm_ctx_var_total",
-    "lddmm_ctx_stream", "lddmm_ctx_launch_config", "lddmm_ctx_launch_shape", "lddmm_objgrd", "lddmm_objgrd_device",
+    "lddmm_ctx_stream", "lddmm_ctx_launch_config", "lddmm_ctx_launch_shape", "lddmm_objgrd", "lddmm_objgrd_device", "lddmm_objgrd_costate",
     "lddmm_lbfgs", "lddmm_lbfgs_device", "lddmm_lbfgs_trace", "lddmm_shoot", "lddmm_LDDMM",
     "lddmm_elm_ifo", "lddmm_multiply_kernel", "lddmm_dq_kernel", "lddmm_varifold",
     "lddmm_flops_per_pair", "lddmm_ctx_time_sweeps", "lddmm_ctx_counters",
@@ -91,6 +91,8 @@ def _load():
     L.lddmm_ctx_launch_shape.argtypes = [C.c_void_p, _ip, C.c_int]
     L.lddmm_objgrd.argtypes = [C.c_void_p, _dp, _dp, _dp]
     L.lddmm_objgrd_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]
+    L.lddmm_objgrd_costate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]
     L.lddmm_lbfgs.argtypes = [C.c_void_p, C.POINTER(Opt), _dp, C.POINTER(Result)]
     L.lddmm_lbfgs_device.argtypes = [C.c_void_p, C.POINTER(Opt), C.c_void_p, C.POINTER(Result)]
     L.lddmm_lbfgs_trace.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]

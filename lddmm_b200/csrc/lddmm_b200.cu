@@ -183,6 +183,7 @@ struct lddmm_ctx {
   int2 *pt_items2 = nullptr;  // (pair, even tile): tiles tile and tile + 1 when present
   int *chunk_pair = nullptr;
   double *X = nullptr, *G = nullptr, *XT = nullptr, *GT = nullptr, *Dv = nullptr;
+  double *pst_out = nullptr;  // costate output of the evaluation in progress (or none)
   double *Sh = nullptr, *Yh = nullptr;
   double *SYm = nullptr, *YYm = nullptr, *coef = nullptr;  // compact-form L-BFGS state
   double *RI = nullptr, *LV = nullptr, *SYd = nullptr, *LU = nullptr;  // long memory
@@ -332,6 +333,7 @@ static cudaError_t adjoint_impl(lddmm_ctx &c, int t, double *g, double *pdot) {
   op.p64 = c.p64;
   op.x64 = c.XT;
   op.g64 = g;
+  op.pst64 = c.pst_out;
   op.us_n = (t > 0) ? c.us + (size_t)((t - 1) & 1) * c.NPtot : nullptr;
   op.ls_n = (t > 0) ? c.ls + (size_t)((t - 1) & 1) * c.NPtot : nullptr;
   op.pdot64 = pdot;
@@ -420,6 +422,7 @@ static cudaError_t adjoint_all_impl(lddmm_ctx &c, double *g) {
   op.x64 = c.XT;
   op.g64 = g;
   op.pdot64 = nullptr;
+  op.pst64 = c.pst_out;
   op.qs0 = c.qs;
   op.as0 = c.as;
   op.us0 = c.us;
@@ -1423,6 +1426,27 @@ extern "C" int lddmm_objgrd_device(lddmm_ctx *ctx, const double *d_alp, double *
     return check_sync(c);
   }
   return 0;
+}
+
+extern "C" int lddmm_objgrd_costate(lddmm_ctx *ctx, const double *d_alp, double *d_fcn,
+                                    double *d_grd, double *d_pst) {
+  if (!ctx || !d_alp || !d_fcn || !d_pst) {
+    set_err("lddmm_objgrd_costate: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  lddmm_ctx &c = *ctx;
+  CU(cudaSetDevice(c.device));
+  CU(reset_sync(c));
+  CU(launch_set_active(c, c.P));
+  CU(load_trial(c, d_alp, false));
+  // the adjoint launches of this evaluation take the output pointer by value; every
+  // other evaluation (and every captured graph) sees none
+  c.pst_out = d_pst;
+  const cudaError_t e = run_eval(c, d_grd ? d_grd : c.GT, d_fcn, nullptr, true);
+  c.pst_out = nullptr;
+  CU(e);
+  CU(cudaStreamSynchronize(c.stream));
+  return check_sync(c);
 }
 
 extern "C" int lddmm_objgrd(lddmm_ctx *ctx, const double *alp, double *fcn, double *grd) {

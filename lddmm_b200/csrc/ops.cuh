@@ -212,6 +212,7 @@ struct AdjointOp {
   float4 *us_n;        // u_{t-1} (written when t > 0)
   float4 *ls_n;        // l_{t-1}
   double *pdot64;      // optional raw dq output [NPtot * D] (standalone dq kernel)
+  double *pst64 = nullptr;  // optional costate output p_{t+1}, variable layout
   int t;
   // bases for the persistent multi-step sweep
   const float4 *qs0, *as0;
@@ -394,6 +395,7 @@ struct AdjointOp {
       const double pdot = P.pd_fac * v[D + d];
       if (pdot64) pdot64[g * D + d] = pdot;
       if (g64) g64[P.var_off + ((size_t)t * P.N + row) * D + d] = P.dt * v[d];
+      if (pst64) pst64[P.var_off + ((size_t)t * P.N + row) * D + d] = F.p[d];
       pn[d] = F.p[d] - P.dt * pdot;
       p64[g * D + d] = pn[d];
     }

@@ -695,7 +695,9 @@ def run_ws_gemm(args):
     lddmm_ws_gemm_bf16 (tcgen05.mma, TMEM accumulator), on the warm-start network's
     layer shapes at a 64-pair batch (2562 points or 5120 triangles per pair), CUDA
     events around each launch with a 256 MiB L2 flush before it; torch's bf16 matmul
-    (cuBLAS) on the same shapes for context.  Prints one JSON line."""
+    (cuBLAS) on the same shapes for context, with FP32 output (torch.mm out_dtype, the
+    same bytes written as ours) and with its default BF16 output (half the output
+    bytes).  Prints one JSON line."""
     import ctypes as C
 
     import torch
@@ -722,8 +724,17 @@ def run_ws_gemm(args):
         def ref():
             torch.matmul(a, b.t())
 
+        def ref32():
+            torch.mm(a, b.t(), out_dtype=torch.float32)
+
+        fns = [("ours", ours), ("torch", ref)]
+        try:
+            ref32()
+            fns.append(("torch32", ref32))
+        except (RuntimeError, TypeError):
+            pass  # no FP32-output bf16 GEMM in this torch build
         res = {}
-        for name, fn in (("ours", ours), ("torch", ref)):
+        for name, fn in fns:
             for _ in range(max(args.warmup, 3)):
                 fn()
             ts = []
@@ -741,6 +752,9 @@ def run_ws_gemm(args):
         err = float((c - torch.matmul(a.float(), b.float().t())).abs().max()
                     / torch.matmul(a.float(), b.float().t()).abs().max())
         out.append({"m": m, "n": n, "k": k, "ours": res["ours"], "torch_bf16": res["torch"],
+                    "torch_bf16_fp32_out": res.get("torch32"),
+                    "hbm_gbs": (m * k * 2 + n * k * 2 + m * n * 4) / (res["ours"]["ms"] * 1e-3)
+                    / 1e9,
                     "frac_of_peak": res["ours"]["tflops"] / peak, "rel_err_vs_fp32": err})
     print(json.dumps({"mode": "ws_gemm", "peak_tflops": peak, "peak_source": peak_src,
                       "shapes": out}), flush=True)

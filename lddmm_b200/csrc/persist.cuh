@@ -106,8 +106,9 @@ __device__ __forceinline__ unsigned int ld_relaxed(const unsigned int *p) {
 // false when the wait timed out (the caller must leave the kernel without departing).
 // `tag` identifies the wait in the error word.  The arrival is a release reduction
 // (the CTA's writes, ordered before it by __syncthreads, become visible with it); the
-// poll is one relaxed load per iteration (the error word is read every 64th); one
-// acquire load after the loop orders the CTA's later reads after the arrivals.
+// poll is one acquire load per iteration (the error word is read every 64th), so the
+// load that sees the count complete also orders the CTA's later reads after the
+// arrivals, with no further round trip to L2.
 __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
                                              unsigned int tag,
                                              unsigned int spin = kSpinLimit) {
@@ -117,7 +118,7 @@ __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
     int ok = 1;
     red_add_release_gpu(&sy->arrive, 1u);
     unsigned int n = 0;
-    while (ld_relaxed(&sy->arrive) < target) {
+    while (ld_acquire(&sy->arrive) < target) {
       if ((++n & 63u) == 0u) {
         if (ld_relaxed(&sy->error) != 0u || n > spin) {
           atomicCAS(&sy->error, 0u, 1u + tag);
@@ -127,9 +128,9 @@ __device__ __forceinline__ bool grid_barrier(StepSync *sy, unsigned int target,
         if (n > 4096u) __nanosleep(64);
       }
     }
-    // acquire: the count read here is the end of the release sequence of every CTA's
-    // arrival (each arrival is a read-modify-write), so their writes are visible
-    if (ok) (void)ld_acquire(&sy->arrive);
+    // the acquire load that read the complete count read the end of the release
+    // sequence of every CTA's arrival (each arrival is a read-modify-write), so their
+    // writes are visible to this thread, and through the __syncthreads to the CTA
     s_ok = ok;
   }
   __syncthreads();

@@ -341,11 +341,20 @@ typedef struct lddmm_ws lddmm_ws;
 int lddmm_ws_create(int n_src, const double *src_nde, int time_steps, int batch_max,
                     int tri_max, double label_scale, unsigned long long seed, void *stream,
                     lddmm_ws **out);
+/* lddmm_ws_create with local target features: every landmark's point input also holds
+ * its local_k (0..27) nearest target triangles (squared centre distance in FP32, ties
+ * to the lower index, nearest first), 7 values each: the centre offset (c - q) * 10,
+ * the unit normal and area * Et / (4 pi).  The point input is then 3 + 64 + 7 local_k
+ * values, padded to a multiple of 16; local_k = 0 is lddmm_ws_create.  Every batch
+ * then needs at least local_k triangles per pair. */
+int lddmm_ws_create_ex(int n_src, const double *src_nde, int time_steps, int batch_max,
+                       int tri_max, double label_scale, unsigned long long seed, int local_k,
+                       void *stream, lddmm_ws **out);
 void lddmm_ws_destroy(lddmm_ws *ws);
 const char *lddmm_ws_last_error(void);
 /* Number of FP32 parameters: per layer (target 1, target 2, point 1, point 2, point 3)
- * Wt[out][in] then b[out], dimensions padded to multiples of 16 (7 -> 16, 67 -> 80,
- * 3T -> round16(3T)); padded entries are zero. */
+ * Wt[out][in] then b[out], dimensions padded to multiples of 16 (7 -> 16,
+ * 67 + 7 local_k -> its multiple of 16, 3T -> round16(3T)); padded entries are zero. */
 long long lddmm_ws_num_params(const lddmm_ws *ws);
 /* Copies the flat parameter vector to (set = 0) or from (set != 0) host memory. */
 int lddmm_ws_params(lddmm_ws *ws, float *host, int set);

@@ -24,7 +24,7 @@ EXPORTS = [
     "lddmm_elm_ifo", "lddmm_multiply_kernel", "lddmm_dq_kernel", "lddmm_varifold",
     "lddmm_flops_per_pair", "lddmm_ctx_time_sweeps", "lddmm_ctx_counters",
     "lddmm_fp32_peak", "lddmm_pipe_peaks", "lddmm_spatial_order", "lddmm_multiply_kernel_noalloc", "lddmm_ctx_timeline",
-    "lddmm_ws_create", "lddmm_ws_destroy", "lddmm_ws_last_error", "lddmm_ws_num_params",
+    "lddmm_ws_create", "lddmm_ws_create_ex", "lddmm_ws_destroy", "lddmm_ws_last_error", "lddmm_ws_num_params",
     "lddmm_ws_params", "lddmm_ws_grad", "lddmm_ws_train_step", "lddmm_ws_predict", "lddmm_ws_backward",
     "lddmm_ws_gemm_bf16", "lddmm_wait_selftest", "lddmm_compute_kernel",
     "lddmm_multiply_kernel2", "lddmm_dq_kernel2", "lddmm_lbfgs_grad",
@@ -128,6 +128,9 @@ def _load():
     _fp = C.POINTER(C.c_float)
     L.lddmm_ws_create.argtypes = [C.c_int, _dp, C.c_int, C.c_int, C.c_int, C.c_double,
                                   C.c_ulonglong, C.c_void_p, C.POINTER(C.c_void_p)]
+    L.lddmm_ws_create_ex.argtypes = [C.c_int, _dp, C.c_int, C.c_int, C.c_int, C.c_double,
+                                     C.c_ulonglong, C.c_int, C.c_void_p,
+                                     C.POINTER(C.c_void_p)]
     L.lddmm_ws_destroy.argtypes = [C.c_void_p]
     L.lddmm_ws_destroy.restype = None
     L.lddmm_ws_last_error.restype = C.c_char_p

@@ -69,7 +69,9 @@ void ws_err(const char *fmt, ...) {
 
 constexpr int kTriIn = 16;   // 7 features, padded
 constexpr int kTriH = 64;
-constexpr int kPtIn = 80;    // 3 + 64, padded
+constexpr int kPtIn = 80;    // 3 + 64, padded (the configured network, no local features)
+constexpr int kMaxLocal = 27;   // nearest triangles per landmark: 3 + 64 + 7 k <= 256
+constexpr float kLocalRel = 10.0f;  // scale of a neighbour's centre offset c_j - q_i
 constexpr int kPtH = 256;
 constexpr int kThreads = 256;
 
@@ -130,21 +132,90 @@ __global__ void maxpool_kernel(const float *h2, int Et, int Etp, float *g, int *
   }
 }
 
-// xp [B * Np][80] = (q_i, g_p, 0) and its transpose
+// The k nearest target triangles of every source landmark: for pair p and landmark i,
+// the indices of the k closest triangle centres in ascending order of the squared
+// distance, computed in FP32 as ((cx - qx)^2 + (cy - qy)^2) + (cz - qz)^2 with every
+// operation rounded (no contraction), ties to the lower index.  One warp per (pair,
+// landmark): lane l keeps the sorted list of its k best among triangles l, l + 32, ...
+// in shared memory, then the warp merges the 32 lists in k rounds of a (distance,
+// index) argmin.  Requires k <= Et.
+constexpr int kKnnWarps = 4;
+__global__ void __launch_bounds__(kKnnWarps * 32)
+    knn_kernel(const float *tri7, int B, int Et, const float *xyz, int N, int k, int *nbr) {
+  __shared__ float s_d[kKnnWarps][kMaxLocal][32];
+  __shared__ int s_i[kKnnWarps][kMaxLocal][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long item = (long long)blockIdx.x * kKnnWarps + warp;
+  if (item >= (long long)B * N) return;  // warp-uniform
+  const int p = (int)(item / N), i = (int)(item - (long long)p * N);
+  const float qx = xyz[i * 3], qy = xyz[i * 3 + 1], qz = xyz[i * 3 + 2];
+  const float *tp = tri7 + (size_t)p * Et * 7;
+  float(*ld)[32] = s_d[warp];
+  int(*li)[32] = s_i[warp];
+  int cnt = 0;
+  for (int j = lane; j < Et; j += 32) {
+    const float dx = __fsub_rn(tp[j * 7], qx), dy = __fsub_rn(tp[j * 7 + 1], qy),
+                dz = __fsub_rn(tp[j * 7 + 2], qz);
+    const float d =
+        __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    if (cnt < k || d < ld[cnt - 1][lane]) {
+      // this lane's candidates come in increasing index, so an equal distance stays
+      // behind the entries already kept
+      int pos = cnt < k ? cnt : k - 1;
+      while (pos > 0 && ld[pos - 1][lane] > d) {
+        ld[pos][lane] = ld[pos - 1][lane];
+        li[pos][lane] = li[pos - 1][lane];
+        --pos;
+      }
+      ld[pos][lane] = d;
+      li[pos][lane] = j;
+      if (cnt < k) ++cnt;
+    }
+  }
+  int h = 0;  // head of this lane's list
+  for (int r = 0; r < k; ++r) {
+    float bd = h < cnt ? ld[h][lane] : INFINITY;
+    int bi = h < cnt ? li[h][lane] : 0x7fffffff;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float od = __shfl_xor_sync(0xffffffffu, bd, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (od < bd || (od == bd && oi < bi)) {
+        bd = od;
+        bi = oi;
+      }
+    }
+    if (h < cnt && li[h][lane] == bi) ++h;  // indices are distinct: one lane advances
+    if (lane == 0) nbr[item * k + r] = bi;
+  }
+}
+
+// xp [B * Np][pt_in] = (q_i, g_p, local features, 0) and its transpose; the local
+// features of neighbour n (nbr, k per landmark; none when k = 0) are the triangle's
+// centre offset (c - q_i) * kLocalRel, unit normal and area * Et / (4 pi)
 __global__ void point_input_kernel(const float *xyz, int N, int Np, int B, const float *g,
+                                   const float *tri7, int Et, const int *nbr, int k, int pt_in,
                                    bf16 *xp, bf16 *xpT) {
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long M = (long long)B * Np;
   if (r >= M) return;
   const int p = (int)(r / Np), i = (int)(r - (long long)p * Np);
-  for (int c = 0; c < kPtIn; ++c) {
+  for (int c = 0; c < pt_in; ++c) {
     float v = 0.0f;
     if (i < N) {
-      if (c < 3) v = xyz[i * 3 + c];
-      else if (c < 3 + kTriH) v = g[p * kTriH + c - 3];
+      if (c < 3) {
+        v = xyz[i * 3 + c];
+      } else if (c < 3 + kTriH) {
+        v = g[p * kTriH + c - 3];
+      } else if (c < 3 + kTriH + 7 * k) {
+        const int n = (c - 3 - kTriH) / 7, f = (c - 3 - kTriH) - 7 * n;
+        const int j = nbr[((size_t)p * N + i) * k + n];
+        const float t = tri7[((size_t)p * Et + j) * 7 + f];
+        v = f < 3 ? __fmul_rn(__fsub_rn(t, xyz[i * 3 + f]), kLocalRel) : t;
+      }
     }
     const bf16 h = __float2bfloat16_rn(v);
-    xp[r * kPtIn + c] = h;
+    xp[r * pt_in + c] = h;
     xpT[(size_t)c * M + r] = h;
   }
 }
@@ -211,7 +282,8 @@ __global__ void rowsum_kernel(const bf16 *xT, long long M, float *out) {
 // pair sums of the first point layer's pre-activation gradient, then through the g
 // columns of P1: dg[p][c] = sum_o (sum_{i of p} da1[p][i][o]) Wt_P1[o][3 + c];
 // block per pair, threads over o
-__global__ void dg_kernel(const bf16 *da1T, long long M, int Np, const float *wt_p1, float *dg) {
+__global__ void dg_kernel(const bf16 *da1T, long long M, int Np, const float *wt_p1, int pt_in,
+                          float *dg) {
   const int p = blockIdx.x;
   __shared__ float s_o[kPtH];
   for (int o = threadIdx.x; o < kPtH; o += blockDim.x) {
@@ -223,7 +295,7 @@ __global__ void dg_kernel(const bf16 *da1T, long long M, int Np, const float *wt
   __syncthreads();
   for (int c = threadIdx.x; c < kTriH; c += blockDim.x) {
     float a = 0.0f;
-    for (int o = 0; o < kPtH; ++o) a = fmaf(s_o[o], wt_p1[o * kPtIn + 3 + c], a);
+    for (int o = 0; o < kPtH; ++o) a = fmaf(s_o[o], wt_p1[o * pt_in + 3 + c], a);
     dg[p * kTriH + c] = a;
   }
 }
@@ -293,6 +365,8 @@ __global__ void predict_out_kernel(const float *y, int ldy, int N, int Np, int B
 struct lddmm_ws {
   int N = 0, Np = 0, T = 0, n_out = 0, n_out_pad = 0, batch_max = 0, et_max = 0, etp_max = 0;
   float label_scale = 1.0f;
+  int local_k = 0, pt_in = kPtIn;  // nearest triangles per landmark; point input width
+  int *nbr = nullptr;              // [batch_max][N][local_k] of the last forward
   int fwd_pairs = 0, fwd_tris = 0;  // batch of the activations of the last prediction
   cudaStream_t stream = nullptr;
   bool own_stream = false;
@@ -507,6 +581,11 @@ int check_batch(lddmm_ws &w, int B, int Et) {
            w.et_max);
     return LDDMM_ERR_ARG;
   }
+  if (Et < w.local_k) {
+    ws_err("%d target triangles, fewer than the %d nearest ones each landmark reads", Et,
+           w.local_k);
+    return LDDMM_ERR_ARG;
+  }
   return 0;
 }
 
@@ -532,9 +611,14 @@ int forward(lddmm_ws &w, const float *tri7, int B, int Et) {
   a.ldo = kTriH;
   WCU(gemm(w, a, 1));
   maxpool_kernel<<<B, 256, 0, w.stream>>>(w.h2, Et, Etp, w.g, w.arg);
+  if (w.local_k > 0) {
+    const long long items = (long long)B * w.N;
+    knn_kernel<<<(unsigned)((items + kKnnWarps - 1) / kKnnWarps), kKnnWarps * 32, 0,
+                 w.stream>>>(tri7, B, Et, w.xyz, w.N, w.local_k, w.nbr);
+  }
   point_input_kernel<<<(unsigned)((Mp + kThreads - 1) / kThreads), kThreads, 0, w.stream>>>(
-      w.xyz, w.N, w.Np, B, w.g, w.xp, w.xpT);
-  a = fwd_args(w.xp, kPtIn, w.L[2], Mp);
+      w.xyz, w.N, w.Np, B, w.g, tri7, Et, w.nbr, w.local_k, w.pt_in, w.xp, w.xpT);
+  a = fwd_args(w.xp, w.pt_in, w.L[2], Mp);
   a.epi = kEpiGelu;
   a.bias = w.params + w.L[2].b_off;
   a.pre_out = w.pre_a1;
@@ -612,7 +696,8 @@ int backward(lddmm_ws &w, int B, int Et, const float *labels, float label_weight
   WCU(gemm(w, a, 1));
   // P1 (its input gradient is needed only in the g columns, summed over each pair)
   WCU(weight_grad(w, w.L[2], w.da1T, w.xpT, Mp));
-  dg_kernel<<<B, 256, 0, w.stream>>>(w.da1T, Mp, w.Np, w.params + w.L[2].w_off, w.dg);
+  dg_kernel<<<B, 256, 0, w.stream>>>(w.da1T, Mp, w.Np, w.params + w.L[2].w_off, w.pt_in,
+                                     w.dg);
   WCU(cudaMemsetAsync(w.dh2, 0, sizeof(bf16) * Mt * kTriH, w.stream));
   WCU(cudaMemsetAsync(w.dh2T, 0, sizeof(bf16) * Mt * kTriH, w.stream));
   unpool_kernel<<<(B * kTriH + kThreads - 1) / kThreads, kThreads, 0, w.stream>>>(
@@ -671,11 +756,13 @@ void adam_step(lddmm_ws &w, double lr) {
 
 extern "C" const char *lddmm_ws_last_error(void) { return g_ws_err.c_str(); }
 
-extern "C" int lddmm_ws_create(int n_src, const double *src_nde, int time_steps, int batch_max,
-                               int tri_max, double label_scale, unsigned long long seed,
-                               void *stream, lddmm_ws **out) {
+extern "C" int lddmm_ws_create_ex(int n_src, const double *src_nde, int time_steps,
+                                  int batch_max, int tri_max, double label_scale,
+                                  unsigned long long seed, int local_k, void *stream,
+                                  lddmm_ws **out) {
   if (!out || n_src < 1 || !src_nde || time_steps < 1 || 3 * time_steps > 256 || batch_max < 1 ||
-      tri_max < 1 || !(label_scale > 0)) {
+      tri_max < 1 || !(label_scale > 0) || local_k < 0 || local_k > kMaxLocal ||
+      local_k > tri_max) {
     ws_err("lddmm_ws_create: bad arguments");
     return LDDMM_ERR_ARG;
   }
@@ -691,6 +778,8 @@ extern "C" int lddmm_ws_create(int n_src, const double *src_nde, int time_steps,
   w->et_max = tri_max;
   w->etp_max = round16(tri_max);
   w->label_scale = (float)label_scale;
+  w->local_k = local_k;
+  w->pt_in = round16(3 + kTriH + 7 * local_k);
   if (stream) {
     w->stream = (cudaStream_t)stream;
   } else {
@@ -699,7 +788,7 @@ extern "C" int lddmm_ws_create(int n_src, const double *src_nde, int time_steps,
   }
   const int dims[5][4] = {{kTriIn, kTriH, 7, kTriH},
                           {kTriH, kTriH, kTriH, kTriH},
-                          {kPtIn, kPtH, 3 + kTriH, kPtH},
+                          {w->pt_in, kPtH, 3 + kTriH + 7 * local_k, kPtH},
                           {kPtH, kPtH, kPtH, kPtH},
                           {kPtH, w->n_out_pad, kPtH, w->n_out}};
   size_t off = 0;
@@ -754,8 +843,9 @@ extern "C" int lddmm_ws_create(int n_src, const double *src_nde, int time_steps,
   WCU(W.alloc(&W.g, (size_t)batch_max * kTriH));
   WCU(W.alloc(&W.dg, (size_t)batch_max * kTriH));
   WCU(W.alloc(&W.arg, (size_t)batch_max * kTriH));
-  WCU(W.alloc(&W.xp, Mp * kPtIn));
-  WCU(W.alloc(&W.xpT, Mp * kPtIn));
+  WCU(W.alloc(&W.xp, Mp * W.pt_in));
+  WCU(W.alloc(&W.xpT, Mp * W.pt_in));
+  WCU(W.alloc(&W.nbr, (size_t)batch_max * n_src * std::max(local_k, 1)));
   for (bf16 **p : {&W.a1, &W.a1T, &W.a2, &W.a2T, &W.da2, &W.da2T, &W.da1, &W.da1T})
     WCU(W.alloc(p, Mp * kPtH));
   WCU(W.alloc(&W.pre_a1, Mp * kPtH));
@@ -774,6 +864,13 @@ extern "C" int lddmm_ws_create(int n_src, const double *src_nde, int time_steps,
   WCU(cudaStreamSynchronize(W.stream));
   *out = guard.release();
   return 0;
+}
+
+extern "C" int lddmm_ws_create(int n_src, const double *src_nde, int time_steps, int batch_max,
+                               int tri_max, double label_scale, unsigned long long seed,
+                               void *stream, lddmm_ws **out) {
+  return lddmm_ws_create_ex(n_src, src_nde, time_steps, batch_max, tri_max, label_scale, seed,
+                            0, stream, out);
 }
 
 extern "C" void lddmm_ws_destroy(lddmm_ws *w) {

@@ -115,14 +115,17 @@ def generate(seeds, batch=64, itr_max=300, rel_obj_tol=1e-6, log=None, make=pair
 
 class WarmStart:
     """The network (C ABI lddmm_ws_*): one source shape, T steps, batches of up to
-    `batch_max` pairs with up to `tri_max` target triangles."""
+    `batch_max` pairs with up to `tri_max` target triangles; `local_k` > 0 adds every
+    landmark's local_k nearest target triangles to its point input
+    (lddmm_ws_create_ex)."""
 
-    def __init__(self, src_nde, T, batch_max, tri_max, label_scale, seed=0, stream=None):
+    def __init__(self, src_nde, T, batch_max, tri_max, label_scale, seed=0, stream=None,
+                 local_k=0):
         src = np.ascontiguousarray(src_nde, dtype=np.float64)
-        self.N, self.T = src.shape[0], T
+        self.N, self.T, self.local_k = src.shape[0], T, local_k
         h = C.c_void_p()
-        check_ws(lib.lddmm_ws_create(self.N, _lib.dptr(src), T, batch_max, tri_max, label_scale,
-                                     seed, stream, C.byref(h)))
+        check_ws(lib.lddmm_ws_create_ex(self.N, _lib.dptr(src), T, batch_max, tri_max,
+                                        label_scale, seed, local_k, stream, C.byref(h)))
         self._h = h
         self.n_params = lib.lddmm_ws_num_params(h)
 
@@ -337,12 +340,13 @@ def evaluate(ws: WarmStart, seeds, batch=64, itr_max=300, rel_obj_tol=1e-6, rel=
 
 
 def experiment(n_train=4096, n_test=512, subdiv=4, epochs=400, batch=64, lr=1e-3, seed=0,
-               log=print, eval_itr_max=1000, eval_rel_obj_tol=1e-9):
+               log=print, eval_itr_max=1000, eval_rel_obj_tol=1e-9, local_k=0):
     """The learned-warm-start workload end to end: plain-method registrations of
     n_train + n_test pairs (training seeds 1000.., held-out seeds 50000..), training,
     then cold vs warm start on the held-out pairs, both run to convergence (relative
     objective change below eval_rel_obj_tol, at most eval_itr_max iterations).
-    Returns a JSON-ready dict."""
+    local_k > 0: the network also reads every landmark's local_k nearest target
+    triangles.  Returns a JSON-ready dict."""
     import functools
 
     import torch
@@ -354,7 +358,7 @@ def experiment(n_train=4096, n_test=512, subdiv=4, epochs=400, batch=64, lr=1e-3
     t_gen = time.perf_counter() - t0
     scale = float(lab.pow(2).mean().sqrt())
     with WarmStart(src, T_STEPS, batch_max=batch, tri_max=tri.shape[1], label_scale=scale,
-                   seed=seed) as ws:
+                   seed=seed, local_k=local_k) as ws:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         hist = train(ws, tri, lab, epochs=epochs, batch=batch, lr=lr, seed=seed)
@@ -364,7 +368,7 @@ def experiment(n_train=4096, n_test=512, subdiv=4, epochs=400, batch=64, lr=1e-3
                       itr_max=eval_itr_max, rel_obj_tol=eval_rel_obj_tol)
     rows = ev.pop("rows")
     ratio = [r["f_start_warm"] / r["f_start_cold"] for r in rows]
-    return dict(n_train=n_train, n_test=n_test, landmarks=int(src.shape[0]),
+    return dict(n_train=n_train, n_test=n_test, local_k=local_k, landmarks=int(src.shape[0]),
                 triangles=int(tri.shape[1]), epochs=epochs, batch=batch, lr=lr,
                 label_rms=scale, seconds_generate=t_gen, seconds_train=t_train,
                 steps=epochs * (n_train // batch), loss_first_epoch=hist[0],
@@ -382,5 +386,9 @@ if __name__ == "__main__":
     ap.add_argument("--test", type=int, default=512)
     ap.add_argument("--subdiv", type=int, default=4)
     ap.add_argument("--epochs", type=int, default=400)
+    ap.add_argument("--local-k", type=int, default=0,
+                    help="nearest target triangles per landmark in the point input (0: the "
+                         "configured network)")
     a = ap.parse_args()
-    print(json.dumps(experiment(a.train, a.test, a.subdiv, a.epochs)), flush=True)
+    print(json.dumps(experiment(a.train, a.test, a.subdiv, a.epochs, local_k=a.local_k)),
+          flush=True)

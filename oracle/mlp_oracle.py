@@ -15,24 +15,58 @@ import numpy as np
 from scipy.special import erf
 
 TRI_IN, TRI_H, PT_IN, PT_H = 16, 64, 80, 256
+LOCAL_REL = np.float32(10.0)  # scale of a neighbour's centre offset
 
 
 def round16(n: int) -> int:
     return (n + 15) // 16 * 16
 
 
-def layer_dims(T: int):
+def pt_in(local_k: int = 0) -> int:
+    """Width of the point input: q, the pooled target features, 7 per neighbour."""
+    return round16(3 + TRI_H + 7 * local_k)
+
+
+def layer_dims(T: int, local_k: int = 0):
     """(in, out) of the five layers, padded."""
-    return [(TRI_IN, TRI_H), (TRI_H, TRI_H), (PT_IN, PT_H), (PT_H, PT_H), (PT_H, round16(3 * T))]
+    return [(TRI_IN, TRI_H), (TRI_H, TRI_H), (pt_in(local_k), PT_H), (PT_H, PT_H),
+            (PT_H, round16(3 * T))]
 
 
-def num_params(T: int) -> int:
-    return sum(o * i + o for i, o in layer_dims(T))
+def num_params(T: int, local_k: int = 0) -> int:
+    return sum(o * i + o for i, o in layer_dims(T, local_k))
 
 
-def unpack(params, T):
+def nearest_triangles(xyz, tri7, k):
+    """(B, N, k) indices of every landmark's k nearest target triangle centres, as the
+    library's knn_kernel: squared distance in FP32, ((dx dx + dy dy) + dz dz) with each
+    operation rounded, ascending, ties to the lower index."""
+    q = np.asarray(xyz, dtype=np.float32)
+    c = np.asarray(tri7, dtype=np.float32)[:, :, :3]
+    d = c[:, None, :, :] - q[None, :, None, :]          # (B, N, Et, 3) FP32
+    d2 = (d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]) + d[..., 2] * d[..., 2]
+    return np.argsort(d2, axis=2, kind="stable")[:, :, :k]
+
+
+def point_inputs(xyz, tri7, g, local_k=0):
+    """(B, N, pt_in) point inputs before BF16 rounding: q, g, then per neighbour
+    (c - q) * 10, the unit normal and area * Et / (4 pi), computed in FP32."""
+    B, N = tri7.shape[0], xyz.shape[0]
+    xp = np.zeros((B, N, pt_in(local_k)))
+    xp[:, :, :3] = xyz[None]
+    xp[:, :, 3:3 + TRI_H] = g[:, None, :]
+    if local_k:
+        nb = nearest_triangles(xyz, tri7, local_k)
+        t = np.asarray(tri7, dtype=np.float32)[np.arange(B)[:, None, None], nb]  # B,N,k,7
+        f = t.copy()
+        f[..., :3] = (t[..., :3] - np.asarray(xyz, dtype=np.float32)[None, :, None, :]) * LOCAL_REL
+        xp[:, :, 3 + TRI_H:3 + TRI_H + 7 * local_k] = f.reshape(B, N, 7 * local_k)
+    return xp
+
+
+def unpack(params, T, local_k=0):
     out, off = [], 0
-    for i, o in layer_dims(T):
+    for i, o in layer_dims(T, local_k):
         Wt = params[off:off + o * i].reshape(o, i)
         off += o * i
         b = params[off:off + o]
@@ -58,7 +92,7 @@ def gelu_grad(x):
 
 
 def loss_and_grad(params, xyz, tri7, labels, T, label_scale, bf=True, label_weight=1.0,
-                  dalpha=None):
+                  dalpha=None, local_k=0):
     """Mean squared error of a batch and the gradient (flat, the library's layout) of
     label_weight * MSE + sum(dalpha * alpha), alpha = label_scale * y the predicted
     momenta.
@@ -67,7 +101,7 @@ def loss_and_grad(params, xyz, tri7, labels, T, label_scale, bf=True, label_weig
     None (no MSE term); dalpha (B, T, N, 3) or None."""
     r = to_bf16 if bf else (lambda v: np.asarray(v, dtype=np.float64))
     params = np.asarray(params, dtype=np.float64)
-    L = unpack(params, T)
+    L = unpack(params, T, local_k)
     B, Et, _ = tri7.shape
     N = xyz.shape[0]
     n_out = 3 * T
@@ -82,10 +116,7 @@ def loss_and_grad(params, xyz, tri7, labels, T, label_scale, bf=True, label_weig
     arg = np.argmax(h2, axis=1)                     # (B, 64): first maximum
     g = np.take_along_axis(h2, arg[:, None, :], axis=1)[:, 0, :]
     # point branch
-    xp = np.zeros((B, N, PT_IN))
-    xp[:, :, :3] = xyz[None]
-    xp[:, :, 3:3 + TRI_H] = g[:, None, :]
-    xp = r(xp)
+    xp = r(point_inputs(xyz, tri7, g, local_k))
     pre1 = xp @ r(P1).T + c1
     a1 = r(gelu(pre1))
     pre2 = a1 @ r(P2).T + c2
@@ -127,12 +158,13 @@ def loss_and_grad(params, xyz, tri7, labels, T, label_scale, bf=True, label_weig
     return loss, np.concatenate(grads)
 
 
-def init_params(T, seed=0):
+def init_params(T, seed=0, local_k=0):
     """Random parameters in the library's layout (real entries only, padding zero)."""
     rng = np.random.default_rng(seed)
-    real = [(7, TRI_H), (TRI_H, TRI_H), (3 + TRI_H, PT_H), (PT_H, PT_H), (PT_H, 3 * T)]
+    real = [(7, TRI_H), (TRI_H, TRI_H), (3 + TRI_H + 7 * local_k, PT_H), (PT_H, PT_H),
+            (PT_H, 3 * T)]
     out = []
-    for (i, o), (ir, orr) in zip(layer_dims(T), real):
+    for (i, o), (ir, orr) in zip(layer_dims(T, local_k), real):
         W = np.zeros((o, i))
         W[:orr, :ir] = rng.uniform(-1, 1, size=(orr, ir)) / np.sqrt(ir)
         b = np.zeros(o)
@@ -141,10 +173,10 @@ def init_params(T, seed=0):
     return np.concatenate(out)
 
 
-def predict(params, xyz, tri7, T, label_scale, bf=True):
+def predict(params, xyz, tri7, T, label_scale, bf=True, local_k=0):
     """Predicted momenta, (B, T, N, 3): the library's lddmm_ws_predict in FP64."""
     r = to_bf16 if bf else (lambda v: np.asarray(v, dtype=np.float64))
-    L = unpack(np.asarray(params, dtype=np.float64), T)
+    L = unpack(np.asarray(params, dtype=np.float64), T, local_k)
     B, Et, _ = tri7.shape
     N = xyz.shape[0]
     (W1, b1), (W2, b2), (P1, c1), (P2, c2), (P3, c3) = L
@@ -152,9 +184,7 @@ def predict(params, xyz, tri7, T, label_scale, bf=True):
     xt[:, :, :7] = tri7
     h1 = r(gelu(r(xt) @ r(W1).T + b1))
     g = (h1 @ r(W2).T + b2).max(axis=1)
-    xp = np.zeros((B, N, PT_IN))
-    xp[:, :, :3] = xyz[None]
-    xp[:, :, 3:3 + TRI_H] = g[:, None, :]
+    xp = point_inputs(xyz, tri7, g, local_k)
     a1 = r(gelu(r(xp) @ r(P1).T + c1))
     a2 = r(gelu(a1 @ r(P2).T + c2))
     y = (a2 @ r(P3).T + c3)[:, :, :3 * T] * label_scale

@@ -116,6 +116,42 @@ def test_predict_vs_oracle(ws_mod):
     assert np.max(np.abs(a - ref)) <= 1e-3 * np.max(np.abs(ref))
 
 
+@pytest.mark.parametrize("local_k", [1, 4, 27])
+def test_local_features_vs_oracle(ws_mod, local_k):
+    """The network with every landmark's local_k nearest target triangles in its point
+    input (lddmm_ws_create_ex): loss, gradient and prediction against the oracle, which
+    finds the neighbours with the same FP32 distances and tie rule."""
+    T, scale = 3, 0.05
+    xyz, tri7, labels = _case(T, seed=3)
+    params = M.init_params(T, seed=9, local_k=local_k).astype(np.float32)
+    t = torch.from_numpy(tri7.astype(np.float32)).cuda()
+    x64 = xyz.astype(np.float32).astype(np.float64)
+    t64 = tri7.astype(np.float32).astype(np.float64)
+    with ws_mod.WarmStart(xyz, T, batch_max=4, tri_max=64, label_scale=scale,
+                          local_k=local_k) as ws:
+        assert ws.n_params == M.num_params(T, local_k)
+        ws.params = params
+        loss, g = ws.grad(t, torch.from_numpy(labels.astype(np.float32)).cuda())
+        a = ws.predict(t).cpu().numpy()
+    lo, go = M.loss_and_grad(params.astype(np.float64), x64, t64,
+                             labels.astype(np.float32).astype(np.float64), T, scale, bf=True,
+                             local_k=local_k)
+    assert abs(loss - lo) <= 1e-4 * abs(lo)
+    assert np.linalg.norm(g - go) / np.linalg.norm(go) < 5e-3
+    ref = M.predict(params.astype(np.float64), x64, t64, T, scale, bf=True,
+                    local_k=local_k).reshape(a.shape)
+    assert np.max(np.abs(a - ref)) <= 1e-3 * np.max(np.abs(ref))
+
+
+def test_local_features_need_enough_triangles(ws_mod):
+    from lddmm_b200 import _lib
+
+    xyz, tri7, _ = _case(3, Et=40)
+    with ws_mod.WarmStart(xyz, 3, batch_max=4, tri_max=64, label_scale=0.05, local_k=8) as ws:
+        with pytest.raises(_lib.LddmmError):
+            ws.predict(torch.from_numpy(tri7[:, :5].astype(np.float32)).contiguous().cuda())
+
+
 def test_training_reduces_loss(ws_mod):
     """Adam steps on a batch whose labels are a smooth function of the landmark
     positions (learnable from the network's inputs)."""

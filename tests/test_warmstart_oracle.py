@@ -81,3 +81,38 @@ def test_outer_gradient_term_finite_differences():
         p2[k] -= h
         fd = (outer(p1) - outer(p2)) / (2 * h)
         assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(g[k])) + 1e-8, (k, fd, g[k])
+
+
+def test_local_features_gradient_finite_differences():
+    """With local target features (local_k = 3) the oracle's FP64 gradient against
+    central differences; the features are inputs, so only the weights move."""
+    T, scale, k = 2, 0.7, 3
+    _, xyz, tri7, labels = _case(T, seed=7)
+    params = M.init_params(T, seed=8, local_k=k)
+    assert params.shape == (M.num_params(T, k),)
+    _, g = M.loss_and_grad(params, xyz, tri7, labels, T, scale, bf=False, local_k=k)
+    rng = np.random.default_rng(9)
+    h = 1e-6
+    for idx in rng.choice(np.flatnonzero(g != 0), 24, replace=False):
+        p1, p2 = params.copy(), params.copy()
+        p1[idx] += h
+        p2[idx] -= h
+        fd = (M.loss_and_grad(p1, xyz, tri7, labels, T, scale, bf=False, local_k=k)[0]
+              - M.loss_and_grad(p2, xyz, tri7, labels, T, scale, bf=False, local_k=k)[0]) / (2 * h)
+        assert abs(fd - g[idx]) <= 1e-6 * max(1.0, abs(g[idx])) + 1e-8, (idx, fd, g[idx])
+
+
+def test_nearest_triangles_order_and_ties():
+    """Nearest first by FP32 squared distance, equal distances to the lower index."""
+    xyz = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0]])
+    cen = np.array([[2.0, 0, 0], [0, 1.0, 0], [0, -1.0, 0], [0.5, 0, 0], [3.0, 0, 0]])
+    tri7 = np.zeros((1, 5, 7))
+    tri7[0, :, :3] = cen
+    nb = M.nearest_triangles(xyz, tri7, 4)
+    assert nb[0, 0].tolist() == [3, 1, 2, 0]      # 0.25, then the tie 1 = 1 (1 before 2)
+    assert nb[0, 1].tolist() == [3, 0, 1, 2]      # 0.25, 1, then the tie 2 = 2
+    rng = np.random.default_rng(3)
+    q, t = rng.normal(size=(20, 3)), rng.normal(size=(2, 30, 7))
+    nb = M.nearest_triangles(q, t, 5)
+    d = ((t[:, None, :, :3] - q[None, :, None, :]) ** 2).sum(-1)
+    assert np.array_equal(nb, np.argsort(d, axis=2)[:, :, :5])

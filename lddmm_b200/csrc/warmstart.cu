@@ -190,33 +190,56 @@ __global__ void __launch_bounds__(kKnnWarps * 32)
   }
 }
 
-// xp [B * Np][pt_in] = (q_i, g_p, local features, 0) and its transpose; the local
-// features of neighbour n (nbr, k per landmark; none when k = 0) are the triangle's
-// centre offset (c - q_i) * kLocalRel, unit normal and area * Et / (4 pi)
+// xp [B * Np][pt_in] = (q_i, g_p, local features, 0) and its transpose: here every
+// column but the local features' (k neighbours x 7, written by local_input_kernel)
 __global__ void point_input_kernel(const float *xyz, int N, int Np, int B, const float *g,
-                                   const float *tri7, int Et, const int *nbr, int k, int pt_in,
-                                   bf16 *xp, bf16 *xpT) {
+                                   int k, int pt_in, bf16 *xp, bf16 *xpT) {
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long M = (long long)B * Np;
   if (r >= M) return;
   const int p = (int)(r / Np), i = (int)(r - (long long)p * Np);
+  const int lo = 3 + kTriH, hi = 3 + kTriH + 7 * k;
   for (int c = 0; c < pt_in; ++c) {
+    if (c == lo) c = hi;  // the local columns
+    if (c >= pt_in) break;
     float v = 0.0f;
     if (i < N) {
-      if (c < 3) {
-        v = xyz[i * 3 + c];
-      } else if (c < 3 + kTriH) {
-        v = g[p * kTriH + c - 3];
-      } else if (c < 3 + kTriH + 7 * k) {
-        const int n = (c - 3 - kTriH) / 7, f = (c - 3 - kTriH) - 7 * n;
-        const int j = nbr[((size_t)p * N + i) * k + n];
-        const float t = tri7[((size_t)p * Et + j) * 7 + f];
-        v = f < 3 ? __fmul_rn(__fsub_rn(t, xyz[i * 3 + f]), kLocalRel) : t;
-      }
+      if (c < 3) v = xyz[i * 3 + c];
+      else if (c < 3 + kTriH) v = g[p * kTriH + c - 3];
     }
     const bf16 h = __float2bfloat16_rn(v);
     xp[r * pt_in + c] = h;
     xpT[(size_t)c * M + r] = h;
+  }
+}
+
+// The local columns of xp / xpT: neighbour n of row r (thread n M + r, rows fastest, so
+// the transposed writes coalesce) is the triangle's centre offset (c - q_i) * kLocalRel,
+// unit normal and area * Et / (4 pi); zeros on padding rows
+__global__ void local_input_kernel(const float *xyz, int N, int Np, int B, const float *tri7,
+                                   int Et, const int *nbr, int k, int pt_in, bf16 *xp,
+                                   bf16 *xpT) {
+  const long long M = (long long)B * Np;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= M * k) return;
+  const int n = (int)(idx / M);
+  const long long r = idx - (long long)n * M;
+  const int p = (int)(r / Np), i = (int)(r - (long long)p * Np);
+  float v[7] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  if (i < N) {
+    const int j = nbr[((size_t)p * N + i) * k + n];
+    const float *t = tri7 + ((size_t)p * Et + j) * 7;
+#pragma unroll
+    for (int f = 0; f < 7; ++f) v[f] = t[f];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) v[f] = __fmul_rn(__fsub_rn(v[f], xyz[i * 3 + f]), kLocalRel);
+  }
+  const int c0 = 3 + kTriH + 7 * n;
+#pragma unroll
+  for (int f = 0; f < 7; ++f) {
+    const bf16 h = __float2bfloat16_rn(v[f]);
+    xp[r * pt_in + c0 + f] = h;
+    xpT[(size_t)(c0 + f) * M + r] = h;
   }
 }
 
@@ -617,7 +640,12 @@ int forward(lddmm_ws &w, const float *tri7, int B, int Et) {
                  w.stream>>>(tri7, B, Et, w.xyz, w.N, w.local_k, w.nbr);
   }
   point_input_kernel<<<(unsigned)((Mp + kThreads - 1) / kThreads), kThreads, 0, w.stream>>>(
-      w.xyz, w.N, w.Np, B, w.g, tri7, Et, w.nbr, w.local_k, w.pt_in, w.xp, w.xpT);
+      w.xyz, w.N, w.Np, B, w.g, w.local_k, w.pt_in, w.xp, w.xpT);
+  if (w.local_k > 0) {
+    const long long n = Mp * w.local_k;
+    local_input_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, w.stream>>>(
+        w.xyz, w.N, w.Np, B, tri7, Et, w.nbr, w.local_k, w.pt_in, w.xp, w.xpT);
+  }
   a = fwd_args(w.xp, w.pt_in, w.L[2], Mp);
   a.epi = kEpiGelu;
   a.bias = w.params + w.L[2].b_off;

@@ -198,22 +198,28 @@ class WarmStart:
         return out
 
 
-def train(ws: WarmStart, tri7, labels, epochs=20, batch=64, lr=1e-3, seed=0, log=None):
-    """Adam over shuffled mini-batches (each pair's rows stay together).  Returns the
-    mean loss of every epoch."""
+def train(ws: WarmStart, tri7, labels, epochs=20, batch=64, lr=1e-3, seed=0, log=None,
+          lr_final=None):
+    """Adam over shuffled mini-batches (each pair's rows stay together), at a constant
+    learning rate, or decayed from lr to lr_final along a half cosine over all steps
+    when lr_final is given.  Returns the mean loss of every epoch."""
     import torch
 
     n = tri7.shape[0]
     g = torch.Generator(device="cpu").manual_seed(seed)
     hist = []
+    steps, step = epochs * (n // batch), 0
     for ep in range(epochs):
         perm = torch.randperm(n, generator=g).cuda()
         tot, cnt = 0.0, 0
         for k in range(0, n - batch + 1, batch):
             idx = perm[k:k + batch]
+            lr_k = lr if lr_final is None else (
+                lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * step / steps)))
             tot += ws.train_step(tri7.index_select(0, idx).contiguous(),
-                                 labels.index_select(0, idx).contiguous(), lr)
+                                 labels.index_select(0, idx).contiguous(), lr_k)
             cnt += 1
+            step += 1
         hist.append(tot / max(cnt, 1))
         if log:
             log(f"epoch {ep + 1}/{epochs}: loss {hist[-1]:.4e}")
@@ -340,13 +346,15 @@ def evaluate(ws: WarmStart, seeds, batch=64, itr_max=300, rel_obj_tol=1e-6, rel=
 
 
 def experiment(n_train=4096, n_test=512, subdiv=4, epochs=400, batch=64, lr=1e-3, seed=0,
-               log=print, eval_itr_max=1000, eval_rel_obj_tol=1e-9, local_k=0):
+               log=print, eval_itr_max=1000, eval_rel_obj_tol=1e-9, local_k=0,
+               gen_itr_max=300, gen_rel_obj_tol=1e-6, lr_final=None):
     """The learned-warm-start workload end to end: plain-method registrations of
     n_train + n_test pairs (training seeds 1000.., held-out seeds 50000..), training,
     then cold vs warm start on the held-out pairs, both run to convergence (relative
     objective change below eval_rel_obj_tol, at most eval_itr_max iterations).
     local_k > 0: the network also reads every landmark's local_k nearest target
-    triangles.  Returns a JSON-ready dict."""
+    triangles.  The training labels are registrations stopped at a relative objective
+    change of gen_rel_obj_tol or gen_itr_max iterations.  Returns a JSON-ready dict."""
     import functools
 
     import torch
@@ -354,21 +362,24 @@ def experiment(n_train=4096, n_test=512, subdiv=4, epochs=400, batch=64, lr=1e-3
     make = functools.partial(pair, src_subdiv=subdiv, tgt_subdiv=subdiv)
     t0 = time.perf_counter()
     tri, lab, src, res = generate(list(range(1000, 1000 + n_train)), batch=batch, make=make,
-                                  log=log)
+                                  log=log, itr_max=gen_itr_max, rel_obj_tol=gen_rel_obj_tol)
     t_gen = time.perf_counter() - t0
     scale = float(lab.pow(2).mean().sqrt())
     with WarmStart(src, T_STEPS, batch_max=batch, tri_max=tri.shape[1], label_scale=scale,
                    seed=seed, local_k=local_k) as ws:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        hist = train(ws, tri, lab, epochs=epochs, batch=batch, lr=lr, seed=seed)
+        hist = train(ws, tri, lab, epochs=epochs, batch=batch, lr=lr, seed=seed,
+                     lr_final=lr_final)
         torch.cuda.synchronize()
         t_train = time.perf_counter() - t0
         ev = evaluate(ws, list(range(50000, 50000 + n_test)), batch=batch, make=make,
                       itr_max=eval_itr_max, rel_obj_tol=eval_rel_obj_tol)
     rows = ev.pop("rows")
     ratio = [r["f_start_warm"] / r["f_start_cold"] for r in rows]
-    return dict(n_train=n_train, n_test=n_test, local_k=local_k, landmarks=int(src.shape[0]),
+    return dict(n_train=n_train, n_test=n_test, local_k=local_k, gen_itr_max=gen_itr_max,
+                gen_rel_obj_tol=gen_rel_obj_tol, lr_final=lr_final,
+                landmarks=int(src.shape[0]),
                 triangles=int(tri.shape[1]), epochs=epochs, batch=batch, lr=lr,
                 label_rms=scale, seconds_generate=t_gen, seconds_train=t_train,
                 steps=epochs * (n_train // batch), loss_first_epoch=hist[0],
@@ -389,6 +400,13 @@ if __name__ == "__main__":
     ap.add_argument("--local-k", type=int, default=0,
                     help="nearest target triangles per landmark in the point input (0: the "
                          "configured network)")
+    ap.add_argument("--label-tol", type=float, default=1e-6,
+                    help="relative objective change at which the label registrations stop")
+    ap.add_argument("--label-itr", type=int, default=300)
+    ap.add_argument("--lr-final", type=float, default=None,
+                    help="decay the learning rate to this value along a half cosine")
     a = ap.parse_args()
-    print(json.dumps(experiment(a.train, a.test, a.subdiv, a.epochs, local_k=a.local_k)),
+    print(json.dumps(experiment(a.train, a.test, a.subdiv, a.epochs, local_k=a.local_k,
+                                gen_itr_max=a.label_itr, gen_rel_obj_tol=a.label_tol,
+                                lr_final=a.lr_final)),
           flush=True)

@@ -274,10 +274,11 @@ def population_leg(stream, local, flush):
             info = {"sweep_ms": {k: round(float(v), 4) for k, v in
                                  ctx.time_sweeps(reps=1).items()},
                     "launch_shape": ctx.launch_shape()}
+            info["reps_ms"] = [round(x, 2) for x in ms]
             return statistics.median(ms), out, cnt, info
 
     with ClockSampler(local) as clk:
-        ms_all, res_all, cnt, info = batch(probs, 2)
+        ms_all, res_all, cnt, info = batch(probs, 3)
     clocks = clk.summary()
     pairs_eval = [2 * P.T * P.nde_num ** 2 + P.dfm_elm_num * (P.dfm_elm_num + P.tgt_elm_num)
                   for P in probs]
@@ -304,7 +305,7 @@ def population_leg(stream, local, flush):
     ref_lbfgs_s = sum(r["ms_lbfgs"] for r in ref) * 1e-3
     ref_total_s = sum(r["ms_total"] for r in ref) * 1e-3
     est_lbfgs_s = sum(len(st) * r["ms_lbfgs"] for st, r in zip(strata, ref)) * 1e-3
-    ms_sample, _, _, _ = batch([probs[k] for k in pick], 2)
+    ms_sample, _, _, _ = batch([probs[k] for k in pick], 3)
     secs = ms_all * 1e-3
     return {
         "workload": POP_WORKLOAD, "pairs": POP_PAIRS,

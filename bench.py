@@ -258,8 +258,9 @@ def population_leg(stream, local, flush):
                     _lib.check(rc)
 
             run(2)  # the context's first L-BFGS call (host-driven cycles)
-            # a whole untimed run: the first full run of a context carries one-time costs
-            # (measured 0.5-1.0 s on the 256-pair batch) that a short call does not reach
+            # a whole untimed run first: inside this bench the first full run of the
+            # 256-pair batch measured 0.5-1.0 s slower than the next ones (standalone the
+            # difference is 0.13 s; the clock sampler starts beside it)
             run(2000)
             ms = []
             for _ in range(reps):

@@ -15,7 +15,7 @@ Measured and asserted, per held-out pair:
     evaluations (no gain; the warm start must not cost more than 5 %); local features
     trained on converged registrations 136.5 vs 235, a median per-pair gain of 1.70x
     (1.43x with the default labels; asserted >= 1.2x).  At full size the same network
-    reaches 2.06x;
+    reaches 2.17x;
   * the result is judged by the plain method, not by the network: the warm run's
     converged objective must match the cold start's within 1e-5 relative.
 The prediction must also start L-BFGS at a clearly lower objective."""

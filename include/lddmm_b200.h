@@ -367,6 +367,14 @@ int lddmm_ws_grad(lddmm_ws *ws, const float *d_tri7, int pairs, int tri_num,
 /* One Adam step (beta 0.9 / 0.999, eps 1e-8) of learning rate lr on one batch. */
 int lddmm_ws_train_step(lddmm_ws *ws, const float *d_tri7, int pairs, int tri_num,
                         const float *d_labels, double lr, double *loss);
+/* A network with local features (local_k > 0): the nearest target triangles of every
+ * landmark of a batch, d_nbr = pairs x n_src x local_k int32 indices (device), as the
+ * forward pass finds them.  Computed once per training pair, they spare the search in
+ * every later step through lddmm_ws_train_step_nbr (same results, bit for bit). */
+int lddmm_ws_neighbours(lddmm_ws *ws, const float *d_tri7, int pairs, int tri_num,
+                        int *d_nbr);
+int lddmm_ws_train_step_nbr(lddmm_ws *ws, const float *d_tri7, int pairs, int tri_num,
+                            const float *d_labels, const int *d_nbr, double lr, double *loss);
 /* Predicted momenta of `pairs` pairs in the variable layout (pairs x T x n_src x 3,
  * FP64), ready as the initial point of lddmm_lbfgs_device.  The activations stay on
  * the context for lddmm_ws_backward until the weights change. */

@@ -25,7 +25,8 @@ EXPORTS = [
     "lddmm_flops_per_pair", "lddmm_ctx_time_sweeps", "lddmm_ctx_counters",
     "lddmm_fp32_peak", "lddmm_pipe_peaks", "lddmm_spatial_order", "lddmm_multiply_kernel_noalloc", "lddmm_ctx_timeline",
     "lddmm_ws_create", "lddmm_ws_create_ex", "lddmm_ws_destroy", "lddmm_ws_last_error", "lddmm_ws_num_params",
-    "lddmm_ws_params", "lddmm_ws_grad", "lddmm_ws_train_step", "lddmm_ws_predict", "lddmm_ws_backward",
+    "lddmm_ws_params", "lddmm_ws_grad", "lddmm_ws_train_step", "lddmm_ws_neighbours", "lddmm_ws_train_step_nbr",
+    "lddmm_ws_predict", "lddmm_ws_backward",
     "lddmm_ws_gemm_bf16", "lddmm_wait_selftest", "lddmm_compute_kernel",
     "lddmm_multiply_kernel2", "lddmm_dq_kernel2", "lddmm_lbfgs_grad",
 ]
@@ -141,6 +142,9 @@ def _load():
     L.lddmm_ws_train_step.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
                                       C.c_double, _dp]
     L.lddmm_ws_predict.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    L.lddmm_ws_neighbours.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+    L.lddmm_ws_train_step_nbr.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                          C.c_void_p, C.c_double, C.POINTER(C.c_double)]
     L.lddmm_ws_backward.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_double,
                                     C.POINTER(C.c_float), C.POINTER(C.c_double)]
     L.lddmm_ws_gemm_bf16.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_longlong,

@@ -613,7 +613,8 @@ int check_batch(lddmm_ws &w, int B, int Et) {
 }
 
 // forward pass; returns through w.y [B * Np][n_out_pad]
-int forward(lddmm_ws &w, const float *tri7, int B, int Et) {
+// nbr_in: the batch's nearest triangles from lddmm_ws_neighbours, or nullptr (searched here)
+int forward(lddmm_ws &w, const float *tri7, int B, int Et, const int *nbr_in = nullptr) {
   const int Etp = round16(Et);
   const long long Mt = (long long)B * Etp, Mp = (long long)B * w.Np;
   tri_input_kernel<<<(unsigned)((Mt + kThreads - 1) / kThreads), kThreads, 0, w.stream>>>(
@@ -634,7 +635,8 @@ int forward(lddmm_ws &w, const float *tri7, int B, int Et) {
   a.ldo = kTriH;
   WCU(gemm(w, a, 1));
   maxpool_kernel<<<B, 256, 0, w.stream>>>(w.h2, Et, Etp, w.g, w.arg);
-  if (w.local_k > 0) {
+  const int *nbr = nbr_in ? nbr_in : w.nbr;
+  if (w.local_k > 0 && !nbr_in) {
     const long long items = (long long)B * w.N;
     knn_kernel<<<(unsigned)((items + kKnnWarps - 1) / kKnnWarps), kKnnWarps * 32, 0,
                  w.stream>>>(tri7, B, Et, w.xyz, w.N, w.local_k, w.nbr);
@@ -644,7 +646,7 @@ int forward(lddmm_ws &w, const float *tri7, int B, int Et) {
   if (w.local_k > 0) {
     const long long n = Mp * w.local_k;
     local_input_kernel<<<(unsigned)((n + kThreads - 1) / kThreads), kThreads, 0, w.stream>>>(
-        w.xyz, w.N, w.Np, B, tri7, Et, w.nbr, w.local_k, w.pt_in, w.xp, w.xpT);
+        w.xyz, w.N, w.Np, B, tri7, Et, nbr, w.local_k, w.pt_in, w.xp, w.xpT);
   }
   a = fwd_args(w.xp, w.pt_in, w.L[2], Mp);
   a.epi = kEpiGelu;
@@ -766,8 +768,8 @@ int backward(lddmm_ws &w, int B, int Et, const float *labels, float label_weight
 
 // forward + loss + backward: gradient in w.grad, loss (mean squared error) in *loss
 int forward_backward(lddmm_ws &w, const float *tri7, int B, int Et, const float *labels,
-                     double *loss) {
-  int rc = forward(w, tri7, B, Et);
+                     double *loss, const int *nbr_in = nullptr) {
+  int rc = forward(w, tri7, B, Et, nbr_in);
   if (rc) return rc;
   return backward(w, B, Et, labels, 1.0f, nullptr, loss);
 }
@@ -943,6 +945,41 @@ extern "C" int lddmm_ws_grad(lddmm_ws *w, const float *d_tri7, int pairs, int tr
                         w->stream));
     WCU(cudaStreamSynchronize(w->stream));
   }
+  return 0;
+}
+
+extern "C" int lddmm_ws_neighbours(lddmm_ws *w, const float *d_tri7, int pairs, int tri_num,
+                                   int *d_nbr) {
+  if (!w || !d_tri7 || !d_nbr || w->local_k < 1) {
+    ws_err("lddmm_ws_neighbours: bad arguments (or a network without local features)");
+    return LDDMM_ERR_ARG;
+  }
+  int rc = check_batch(*w, pairs, tri_num);
+  if (rc) return rc;
+  const long long items = (long long)pairs * w->N;
+  knn_kernel<<<(unsigned)((items + kKnnWarps - 1) / kKnnWarps), kKnnWarps * 32, 0,
+               w->stream>>>(d_tri7, pairs, tri_num, w->xyz, w->N, w->local_k, d_nbr);
+  WCU(cudaGetLastError());
+  WCU(cudaStreamSynchronize(w->stream));
+  return 0;
+}
+
+extern "C" int lddmm_ws_train_step_nbr(lddmm_ws *w, const float *d_tri7, int pairs,
+                                       int tri_num, const float *d_labels, const int *d_nbr,
+                                       double lr, double *loss) {
+  if (!w || !d_tri7 || !d_labels || !(lr > 0) || (w->local_k > 0 && !d_nbr)) {
+    ws_err("lddmm_ws_train_step_nbr: bad arguments");
+    return LDDMM_ERR_ARG;
+  }
+  int rc = check_batch(*w, pairs, tri_num);
+  if (rc) return rc;
+  w->fwd_pairs = 0;
+  rc = forward_backward(*w, d_tri7, pairs, tri_num, d_labels, loss,
+                        w->local_k > 0 ? d_nbr : nullptr);
+  if (rc) return rc;
+  adam_step(*w, lr);
+  WCU(cudaGetLastError());
+  WCU(refresh_bf16(*w));
   return 0;
 }
 

@@ -167,12 +167,35 @@ class WarmStart:
                                    g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)))
         return loss.value, g
 
-    def train_step(self, tri7, labels, lr=1e-3):
+    def train_step(self, tri7, labels, lr=1e-3, nbr=None):
+        """One Adam step; nbr: the batch's neighbours from neighbours() (networks with
+        local features: spares the search, same result)."""
         loss = C.c_double()
-        check_ws(lib.lddmm_ws_train_step(self._h, C.c_void_p(tri7.data_ptr()), tri7.shape[0],
-                                         tri7.shape[1], C.c_void_p(labels.data_ptr()), lr,
-                                         C.byref(loss)))
+        if nbr is None:
+            check_ws(lib.lddmm_ws_train_step(self._h, C.c_void_p(tri7.data_ptr()),
+                                             tri7.shape[0], tri7.shape[1],
+                                             C.c_void_p(labels.data_ptr()), lr,
+                                             C.byref(loss)))
+        else:
+            check_ws(lib.lddmm_ws_train_step_nbr(self._h, C.c_void_p(tri7.data_ptr()),
+                                                 tri7.shape[0], tri7.shape[1],
+                                                 C.c_void_p(labels.data_ptr()),
+                                                 C.c_void_p(nbr.data_ptr()), lr,
+                                                 C.byref(loss)))
         return loss.value
+
+    def neighbours(self, tri7, batch=64):
+        """(pairs, N, local_k) int32 device tensor: every landmark's nearest target
+        triangles, searched in chunks of `batch` pairs."""
+        import torch
+
+        out = torch.empty((tri7.shape[0], self.N, self.local_k), dtype=torch.int32,
+                          device="cuda")
+        for k in range(0, tri7.shape[0], batch):
+            t = tri7[k:k + batch].contiguous()
+            check_ws(lib.lddmm_ws_neighbours(self._h, C.c_void_p(t.data_ptr()), t.shape[0],
+                                             t.shape[1], C.c_void_p(out[k:k + batch].data_ptr())))
+        return out
 
     def backward(self, labels=None, label_weight=1.0, dalpha=None, lr=0.0, want_grad=False):
         """Backward pass of the last predict()'s batch for the loss
@@ -209,6 +232,8 @@ def train(ws: WarmStart, tri7, labels, epochs=20, batch=64, lr=1e-3, seed=0, log
     g = torch.Generator(device="cpu").manual_seed(seed)
     hist = []
     steps, step = epochs * (n // batch), 0
+    # networks with local features: every pair's neighbours once, not in every step
+    nbr = ws.neighbours(tri7, batch) if getattr(ws, "local_k", 0) else None
     for ep in range(epochs):
         perm = torch.randperm(n, generator=g).cuda()
         tot, cnt = 0.0, 0
@@ -217,7 +242,8 @@ def train(ws: WarmStart, tri7, labels, epochs=20, batch=64, lr=1e-3, seed=0, log
             lr_k = lr if lr_final is None else (
                 lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * step / steps)))
             tot += ws.train_step(tri7.index_select(0, idx).contiguous(),
-                                 labels.index_select(0, idx).contiguous(), lr_k)
+                                 labels.index_select(0, idx).contiguous(), lr_k,
+                                 None if nbr is None else nbr.index_select(0, idx).contiguous())
             cnt += 1
             step += 1
         hist.append(tot / max(cnt, 1))

@@ -143,6 +143,31 @@ def test_local_features_vs_oracle(ws_mod, local_k):
     assert np.max(np.abs(a - ref)) <= 1e-3 * np.max(np.abs(ref))
 
 
+def test_cached_neighbours_train_bit_for_bit(ws_mod):
+    """lddmm_ws_neighbours finds the oracle's neighbours, and training steps that take
+    them (lddmm_ws_train_step_nbr) give the same losses and weights, bit for bit, as
+    steps that search themselves."""
+    T, scale, k = 3, 0.05, 4
+    xyz, tri7, labels = _case(T, seed=5)
+    params = M.init_params(T, seed=10, local_k=k).astype(np.float32)
+    t = torch.from_numpy(tri7.astype(np.float32)).cuda()
+    y = torch.from_numpy(labels.astype(np.float32)).cuda()
+    runs = []
+    for cached in (False, True):
+        with ws_mod.WarmStart(xyz, T, batch_max=4, tri_max=64, label_scale=scale,
+                              local_k=k) as ws:
+            ws.params = params
+            nbr = None
+            if cached:
+                nbr = ws.neighbours(t)
+                ref = M.nearest_triangles(xyz.astype(np.float32), tri7.astype(np.float32), k)
+                assert np.array_equal(nbr.cpu().numpy(), ref)
+            losses = [ws.train_step(t, y, 1e-3, nbr) for _ in range(3)]
+            runs.append((losses, ws.params))
+    assert runs[0][0] == runs[1][0]
+    assert np.array_equal(runs[0][1], runs[1][1])
+
+
 def test_local_features_need_enough_triangles(ws_mod):
     from lddmm_b200 import _lib
 

@@ -221,6 +221,14 @@ class WarmStart:
         return out
 
 
+def lr_at(step, steps, lr, lr_final=None):
+    """Learning rate of training step `step` of `steps`: lr throughout, or a half
+    cosine from lr (step 0) down to lr_final (step `steps`)."""
+    if lr_final is None:
+        return lr
+    return lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * step / steps))
+
+
 def train(ws: WarmStart, tri7, labels, epochs=20, batch=64, lr=1e-3, seed=0, log=None,
           lr_final=None):
     """Adam over shuffled mini-batches (each pair's rows stay together), at a constant
@@ -239,8 +247,7 @@ def train(ws: WarmStart, tri7, labels, epochs=20, batch=64, lr=1e-3, seed=0, log
         tot, cnt = 0.0, 0
         for k in range(0, n - batch + 1, batch):
             idx = perm[k:k + batch]
-            lr_k = lr if lr_final is None else (
-                lr_final + 0.5 * (lr - lr_final) * (1.0 + math.cos(math.pi * step / steps)))
+            lr_k = lr_at(step, steps, lr, lr_final)
             tot += ws.train_step(tri7.index_select(0, idx).contiguous(),
                                  labels.index_select(0, idx).contiguous(), lr_k,
                                  None if nbr is None else nbr.index_select(0, idx).contiguous())

@@ -142,3 +142,16 @@ def test_population_workers_build_the_same_pairs():
     for x, y in zip(a, b):
         assert np.array_equal(x.ini_nde, y.ini_nde) and np.array_equal(x.elm_vtx, y.elm_vtx)
         assert np.array_equal(x.tgt_cen, y.tgt_cen) and np.array_equal(x.elm_ifo, y.elm_ifo)
+
+
+def test_warm_start_learning_rate_schedule():
+    """Constant without lr_final; with it a half cosine from lr to lr_final, halfway at
+    the middle step, monotone."""
+    from lddmm_b200.warmstart import lr_at
+
+    assert lr_at(0, 100, 1e-3) == lr_at(99, 100, 1e-3) == 1e-3
+    assert lr_at(0, 100, 1e-3, 1e-5) == pytest.approx(1e-3)
+    assert lr_at(100, 100, 1e-3, 1e-5) == pytest.approx(1e-5)
+    assert lr_at(50, 100, 1e-3, 1e-5) == pytest.approx(0.5 * (1e-3 + 1e-5))
+    seq = [lr_at(k, 100, 1e-3, 1e-5) for k in range(101)]
+    assert all(a >= b for a, b in zip(seq, seq[1:]))
